@@ -1,0 +1,343 @@
+"""Benchmark of the multislice hot path on B200.
+
+Workload (default, --config cbed): batched convergent-beam diffraction with
+frozen phonons -- Si [001] 16x16x60 cells, 1024^2 sampling, 240 slices of
+1.358 A, 300 kV, 20 mrad probe centred, 8 phonon configurations in one call.
+One step = one full simulation (8 configurations x 240 slices = 1920
+probe-slices).  Metric: probe*slice/s (higher is better).
+
+  value : device-timed with CUDA events on the engine's stream; the pattern
+          stays in HBM; atoms are handed over from host memory each step
+          (3 MB) as part of the call.
+  e2e   : the same public C-ABI call with host buffers, host->device atoms
+          and device->host pattern inside every step, wall-clocked.
+
+Multi-GPU (torchrun): each rank simulates its own 8 phonon configurations
+(seed offset by rank) and the patterns are summed with one NCCL all-reduce
+per step; weak scaling, time = max over ranks.
+
+--impl reference times the reference's CPU implementation of the path, which
+here is the FP64 C restatement under oracle/ (the reference itself has no CPU
+path and does not build), on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALGO_BYTES_NOTE = ("per probe-slice: one FP32-complex read + write of the wave (16 N bytes) plus the FP32 potential "
+                   "slice amortised over the waves sharing it (4 N / S)")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cbed", choices=["cbed", "stem", "hrtem"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(config: str, rank: int = 0):
+    from cudaem_b200 import workloads as wl
+    if config == "cbed":
+        p, at = wl.cbed_si()
+        p.pn_seed = 42 + 1000 * rank
+        units = p.pn_nconf * 240
+        desc = {"workload": "CBED Si[001] 16x16x60 cells, 1024^2, 240 slices x 1.358 A, 300 kV, 20 mrad, "
+                            "8 frozen-phonon configurations per call", "grid": 1024, "slices": 240,
+                "phonon_configs": 8, "waves_per_potential": 1}
+    elif config == "stem":
+        p, at = wl.stem_sto(nconf=1, scan=(16, 16))
+        units = 16 * 16 * 50
+        desc = {"workload": "STEM ADF SrTiO3[001] 16x16x25 cells, 1024^2, 50 slices, 200 kV, 22 mrad, "
+                            "16x16 probe positions of the 64x64 scan, one phonon configuration", "grid": 1024,
+                "slices": 50, "probes": 256, "waves_per_potential": 256}
+    else:
+        p, at = wl.hrtem_sto()
+        units = 40
+        desc = {"workload": "HRTEM SrTiO3[001] 10x10x20 cells, 512^2, 40 slices, 200 kV plane wave + CTF",
+                "grid": 512, "slices": 40, "waves_per_potential": 1}
+    return p, at, units, desc
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(config: str, p_full, budget_s: float = 20.0):
+    """The FP64 oracle on a bounded sample of the same workload, all host threads."""
+    from cudaem_b200 import workloads as wl
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    if config == "cbed":
+        p, at = wl.cbed_si(cells=(16, 16, 10), nconf=1)
+        sample = "1 phonon configuration x 40 slices of the 1024^2 Si CBED workload (16x16x10 cells)"
+        t = time.perf_counter()
+        orc.simulate_cbed(p, at)
+        dt = time.perf_counter() - t
+        _, _, units_per = 1, 1, 40
+        units = 40
+    elif config == "stem":
+        p, at = wl.stem_sto(nconf=1, scan=(2, 1))
+        sample = "2 probes x 50 slices of the 1024^2 SrTiO3 STEM workload"
+        t = time.perf_counter()
+        orc.simulate_stem(p, at)
+        dt = time.perf_counter() - t
+        units = 2 * 50
+    else:
+        p, at = wl.hrtem_sto()
+        sample = "the full 512^2 HRTEM workload (40 slices)"
+        t = time.perf_counter()
+        orc.simulate_tem(p, at)
+        dt = time.perf_counter() - t
+        units = 40
+    return {"value": units / dt, "unit": "probe*slice/s", "cores": threads, "kind": "port", "sample": sample,
+            "seconds": dt}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cudaem_b200 import workloads as wl  # noqa: F401
+    from oracle import oracle as orc
+    orc.build()
+    _, _, _, desc = workload(args.config)
+    times, units = [], 0
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(args.config, None)
+        if i >= args.warmup:
+            times.append(r["seconds"])
+            units = r["value"] * r["seconds"]
+    tot = sum(times)
+    val = units * len(times) / tot
+    line = {"impl": "reference", "metric": "probe*slice/s", "value": val, "unit": "probe*slice/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": desc,
+            "cpu_baseline": {"value": val, "unit": "probe*slice/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": val, "unit": "probe*slice/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+
+    import cudaem_b200 as cb
+    from cudaem_b200 import _abi as abi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    p, at, units, desc = workload(args.config, rank)
+    ctx = cb.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    L = cb.lib()
+    N = p.nx * p.ny
+    out_dev = torch.empty((p.ny, p.nx), dtype=torch.float32, device="cuda")
+    co = abi.ms_output()
+    cp, ca = p.c(), at.c()
+    is_stem = args.config == "stem"
+    if is_stem:
+        out_dev = torch.empty((p.n_det, p.scan_ny, p.scan_nx), dtype=torch.float32, device="cuda")
+        co.stem_intensity = C.cast(C.c_void_p(out_dev.data_ptr()), C.POINTER(C.c_float))
+    else:
+        co.image_intensity = C.cast(C.c_void_p(out_dev.data_ptr()), C.POINTER(C.c_float))
+    co.on_device = 1
+    fn = {"cbed": L.ms_simulate_cbed, "stem": L.ms_simulate_stem, "hrtem": L.ms_simulate_tem}[args.config]
+
+    def step(o):
+        ctx.check(fn(ctx.handle, C.byref(cp), C.byref(ca), C.byref(o)))
+        if dist is not None:
+            dist.all_reduce(out_dev)
+
+    for _ in range(args.warmup):
+        step(co)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(co)
+            launches += ctx.last_launch_count
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = units * world * args.steps / (ms / 1e3)
+
+    # end to end: host atoms in, host pattern out, wall clock around the public call
+    host_out = np.empty(tuple(out_dev.shape), np.float32)
+    ch = abi.ms_output()
+    if is_stem:
+        ch.stem_intensity = host_out.ctypes.data_as(C.POINTER(C.c_float))
+    else:
+        ch.image_intensity = host_out.ctypes.data_as(C.POINTER(C.c_float))
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.check(fn(ctx.handle, C.byref(cp), C.byref(ca), C.byref(ch)))
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = units * world * args.steps / e2e_s
+    h2d = at.n * (4 * 6)
+    d2h = host_out.nbytes
+
+    # dominant kernel: per-launch device time from events around each launch (profiling run)
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    step(co)
+    torch.cuda.synchronize()
+    prof = {k: ctx.profile(k) for k in ("row", "col", "potential", "probe")}
+    ctx.set_profiling(False)
+    dom = max(prof, key=lambda k: prof[k][1])
+    n_l, tot_ms = prof[dom]
+    waves = p.pn_nconf if args.config == "cbed" else (p.scan_nx * p.scan_ny if is_stem else 1)
+    S_share = desc.get("waves_per_potential", 1)
+    if dom in ("row", "col"):
+        # one launch = one pass over the wave batch; algorithmic bytes per wave: read + write 8 N, plus
+        # (row pass) the potential slice 4 N shared by S waves
+        per_wave = 16 * N + (4 * N / S_share if dom == "row" else 0)
+        algo = per_wave * waves
+    else:
+        algo = 4 * N * (p.pn_nconf if args.config == "cbed" else 1)
+    avg_s = tot_ms / max(1, n_l) / 1e3
+    achieved = algo / avg_s / 1e9
+    peak, peak_kind = peaks()
+    hbm_traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            hbm_traffic = json.load(f).get(f"{args.config}:{dom}")
+    except Exception:
+        pass
+    line = {"metric": "probe*slice/s", "value": value, "unit": "probe*slice/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32-complex (fp64 phases)", "data": "synthetic",
+            "config": dict(desc, l2="inputs larger than L2 (potential store of every slice, >7 GB)",
+                           parallelism=f"phonon configurations per rank, {world} rank(s)"),
+            "e2e": {"value": e2e, "unit": "probe*slice/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": hbm_traffic,
+                         "launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": algo,
+                         "kernel_share": {k: v[1] for k, v in prof.items()}},
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.config, p)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,57 @@
+// The context behind the opaque ms_ctx handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+struct ms_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    bool constants_ready = false;
+
+    struct Buf {
+        void* p = nullptr;
+        size_t bytes = 0;
+    };
+    std::map<std::string, Buf> bufs;             // device buffers reused across calls
+    std::map<int, void*> twiddles;               // inter-level FFT twiddles per transform length
+    std::map<std::string, msb::ElemTable> elem_cache;
+
+    // per-kernel event timing
+    bool profile = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<std::string, size_t>> ev_pending;  // kernel class, index of its start event
+    std::map<std::string, std::pair<int64_t, double>> prof;   // launches, total ms
+    cudaEvent_t prof_event();
+    void prof_resolve();
+
+    // A device buffer of at least `bytes`, kept for later calls.  Growing a buffer first
+    // drains the stream so that no queued kernel still reads the old allocation.
+    void* buf(const std::string& name, size_t bytes);
+    void release_all();
+};
+
+namespace msb {
+void ctx_activate(ms_ctx* c);
+void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed);
+void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out);
+void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out);
+void sim_potential(ms_ctx* c, const ms_params& p, const ms_atoms& a, int conf, float* V, int64_t cap, int on_dev,
+                   int* n_slices);
+void sim_stem_forward_potential(ms_ctx* c, const ms_params& p, const float* V, int S, int on_dev, double z_init,
+                                const double* xy, int np, float* I);
+void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int on_dev, double z_init,
+                       const double* xy, int np, const float* target, double* loss, float* dV, double* dC10,
+                       double* dC30);
+void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_output* outs, double* lat);
+}  // namespace msb

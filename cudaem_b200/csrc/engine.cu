@@ -1,0 +1,903 @@
+// Mode drivers of the engine: the specimen pipeline on the device and the
+// HRTEM/ED, CBED, STEM and thickness loops over the fused slice passes.
+//
+// Call structure (one blocking C-ABI call):
+//   upload atoms -> displace every configuration of a group (device) ->
+//   z range (one small device-to-host read) -> slicing planes (host, bit-exact
+//   with the device) -> slice assignment + stable radix sort + gather (device)
+//   -> projected potentials of all slices of the group (device) ->
+//   probe / plane wave -> per slice: row pass, column pass -> post passes ->
+//   FP64 accumulation over configurations -> output.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "ctx.hpp"
+#include "detmath.cuh"
+#include "fft_layout.hpp"
+#include "kernels.cuh"
+
+#define CK(x)                                                                                              \
+    do {                                                                                                   \
+        cudaError_t e_ = (x);                                                                              \
+        if (e_ != cudaSuccess)                                                                             \
+            throw ::msb::MsError(e_ == cudaErrorMemoryAllocation ? MS_ERR_OUT_OF_MEMORY : MS_ERR_CUDA,     \
+                                 std::string(#x) + ": " + cudaGetErrorString(e_));                         \
+    } while (0)
+
+void* ms_ctx::buf(const std::string& name, size_t bytes)
+{
+    Buf& b = bufs[name];
+    if (b.p && b.bytes >= bytes) return b.p;
+    if (b.p) {
+        cudaStreamSynchronize(stream);
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    size_t want = std::max<size_t>(bytes, 256);
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw msb::MsError(MS_ERR_OUT_OF_MEMORY,
+                           "device allocation of " + std::to_string(want) + " bytes for '" + name + "' failed");
+    }
+    b.p = p;
+    b.bytes = want;
+    return p;
+}
+
+void ms_ctx::release_all()
+{
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& kv : bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    bufs.clear();
+    for (auto& kv : twiddles) cudaFree(kv.second);
+    twiddles.clear();
+}
+
+cudaEvent_t ms_ctx::prof_event()
+{
+    if (ev_used == ev_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) throw msb::MsError(MS_ERR_CUDA, "event creation failed");
+        ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
+}
+
+void ms_ctx::prof_resolve()
+{
+    for (auto& pe : ev_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev_pool[pe.second], ev_pool[pe.second + 1]) == cudaSuccess) {
+            auto& a = prof[pe.first];
+            a.first += 1;
+            a.second += ms;
+        }
+    }
+    ev_pending.clear();
+    ev_used = 0;
+}
+
+namespace msb {
+
+namespace {
+// Launch wrappers: with profiling on, each launch sits between two events on the context stream.
+template <class F>
+void timed(ms_ctx* c, const char* cls, F&& launch)
+{
+    if (!c->profile) {
+        launch();
+        return;
+    }
+    size_t i0 = c->ev_used;
+    cudaEvent_t a = c->prof_event();
+    cudaEvent_t b = c->prof_event();
+    cudaEventRecord(a, c->stream);
+    launch();
+    cudaEventRecord(b, c->stream);
+    c->ev_pending.emplace_back(cls, i0);
+}
+
+void run_row(ms_ctx* c, int N, int op, const PassArgs& a, int nw, int ny, cudaStream_t st)
+{
+    timed(c, "row", [&] { launch_row(N, op, a, nw, ny, st); });
+}
+
+void run_col(ms_ctx* c, int N, int op, const PassArgs& a, int nw, int nx, cudaStream_t st)
+{
+    timed(c, op == COL_PROBE_INV ? "probe" : "col", [&] { launch_col(N, op, a, nw, nx, st); });
+}
+
+void run_potential(ms_ctx* c, const PotArgs& a, int n_conf, cudaStream_t st)
+{
+    timed(c, "potential", [&] { launch_potential(a, n_conf, st); });
+}
+}  // namespace
+
+namespace {
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+int team_size(int N)
+{
+    switch (N) {
+    case 128: return FftCfg<128>::G;
+    case 256: return FftCfg<256>::G;
+    case 512: return FftCfg<512>::G;
+    case 1024: return FftCfg<1024>::G;
+    case 2048: return FftCfg<2048>::G;
+    }
+    throw MsError(MS_ERR_UNSUPPORTED, "unsupported transform length");
+}
+
+const float2* twiddles(ms_ctx* c, int N)
+{
+    auto it = c->twiddles.find(N);
+    if (it != c->twiddles.end()) return (const float2*)it->second;
+    int G = team_size(N), E = N / G;
+    std::vector<float2> t((size_t)N);
+    for (int k1 = 0; k1 < E; k1++)
+        for (int g = 0; g < G; g++) {
+            double a = -2.0 * kPi * (double)((int64_t)g * k1 % N) / (double)N;
+            t[(size_t)k1 * G + g] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+    void* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(float2) * N));
+    CK(cudaMemcpy(p, t.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+    c->twiddles[N] = p;
+    return (const float2*)p;
+}
+
+LensDev lens_dev(const LensCoef& L)
+{
+    LensDev d;
+    std::memset(&d, 0, sizeof(d));
+    d.m = L.m;
+    d.phi_req = L.phi_req;
+    d.cc10 = L.cc10; d.cc12 = L.cc12; d.cc21 = L.cc21; d.cc23 = L.cc23; d.cc30 = L.cc30; d.cc32 = L.cc32;
+    d.cc34 = L.cc34; d.cc41 = L.cc41; d.cc43 = L.cc43; d.cc45 = L.cc45; d.cc50 = L.cc50; d.cc52 = L.cc52;
+    d.cc54 = L.cc54; d.cc56 = L.cc56;
+    d.p12 = L.p12; d.p21 = L.p21; d.p23 = L.p23; d.p32 = L.p32; d.p34 = L.p34; d.p41 = L.p41; d.p43 = L.p43;
+    d.p45 = L.p45; d.p52 = L.p52; d.p54 = L.p54; d.p56 = L.p56;
+    d.g2min = L.g2min;
+    d.g2max = L.g2max;
+    return d;
+}
+
+struct Setup {
+    Physics ph;
+    GridConst gc;
+    GridDev gd;
+    const float2* tw_x;
+    const float2* tw_y;
+    const float2* prop_x;
+    const float2* prop_y;
+    int64_t N;
+};
+
+Setup make_setup(ms_ctx* c, const ms_params& p)
+{
+    Setup s;
+    s.ph = physics_of(p.E0, p.theta);
+    s.gc = grid_of(p, s.ph);
+    s.N = (int64_t)p.nx * p.ny;
+    s.gd.nx = p.nx;
+    s.gd.ny = p.ny;
+    s.gd.dgx_f = s.gc.dgx_f;
+    s.gd.dgy_f = s.gc.dgy_f;
+    s.gd.dgx = s.gc.dgx;
+    s.gd.dgy = s.gc.dgy;
+    s.gd.gl2_f = (float)s.gc.gl2;
+    s.gd.alpha_f = (float)s.gc.alpha;
+    s.gd.bwl = p.bwl ? 1 : 0;
+    s.gd.inv_n = 1.0f / (float)s.N;
+    s.tw_x = twiddles(c, p.nx);
+    s.tw_y = twiddles(c, p.ny);
+    // separable propagator phase exp(i w (g - g0)^2) per axis, formed in FP64 (device_kernels.cuh:215-234)
+    std::vector<float2> px(p.nx), py(p.ny);
+    for (int i = 0; i < p.nx; i++) {
+        double g = (double)((i < p.nx / 2) ? i : i - p.nx) * s.gc.dgx - s.gc.g0x;
+        double th = s.gc.prop_w * g * g;
+        px[i] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+    for (int i = 0; i < p.ny; i++) {
+        double g = (double)((i < p.ny / 2) ? i : i - p.ny) * s.gc.dgy - s.gc.g0y;
+        double th = s.gc.prop_w * g * g;
+        py[i] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+    float2* dpx = (float2*)c->buf("prop_x", sizeof(float2) * p.nx);
+    float2* dpy = (float2*)c->buf("prop_y", sizeof(float2) * p.ny);
+    CK(cudaMemcpyAsync(dpx, px.data(), sizeof(float2) * p.nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dpy, py.data(), sizeof(float2) * p.ny, cudaMemcpyHostToDevice, c->stream));
+    s.prop_x = dpx;
+    s.prop_y = dpy;
+    return s;
+}
+
+// Atoms on the device plus one radial spline table per distinct element.
+struct AtomsDev {
+    int64_t n;
+    const float *x, *y, *z, *sig, *occ;
+    const int* elem;
+    const ElemTable* tables;
+    int n_elem;
+};
+
+std::string elem_key(const ms_params& p, int Z)
+{
+    std::string k = std::to_string(Z) + "|" + std::to_string(p.potential_type) + "|" + std::to_string(p.pot_rmin) +
+                    "|" + std::to_string(p.pot_rmax);
+    for (int i = 0; i < p.n_element_coefs; i++)
+        if (p.element_coefs[i].Z == Z) {
+            k += "|" + std::to_string(p.element_coefs[i].form);
+            for (int j = 0; j < MS_MAX_COEF; j++)
+                k += "," + std::to_string(p.element_coefs[i].cl[j]) + "," + std::to_string(p.element_coefs[i].cnl[j]);
+        }
+    return k;
+}
+
+AtomsDev upload_atoms(ms_ctx* c, const ms_params& p, const ms_atoms& a)
+{
+    AtomsDev d;
+    d.n = a.n;
+    std::vector<int> zs(a.Z, a.Z + a.n);
+    std::sort(zs.begin(), zs.end());
+    zs.erase(std::unique(zs.begin(), zs.end()), zs.end());
+    MS_REQUIRE(zs.size() <= 16, MS_ERR_UNSUPPORTED, "at most 16 distinct elements per specimen");
+    std::vector<ElemTable> tabs(zs.size());
+    for (size_t i = 0; i < zs.size(); i++) {
+        std::string k = elem_key(p, zs[i]);
+        auto it = c->elem_cache.find(k);
+        if (it == c->elem_cache.end()) {
+            ElemTable t;
+            build_elem_table(p, zs[i], &t);
+            it = c->elem_cache.emplace(k, t).first;
+        }
+        tabs[i] = it->second;
+    }
+    std::vector<int> el(a.n);
+    for (int64_t i = 0; i < a.n; i++) el[i] = (int)(std::lower_bound(zs.begin(), zs.end(), a.Z[i]) - zs.begin());
+    size_t fb = sizeof(float) * (size_t)a.n;
+    float* x = (float*)c->buf("at_x", fb);
+    float* y = (float*)c->buf("at_y", fb);
+    float* z = (float*)c->buf("at_z", fb);
+    float* sg = (float*)c->buf("at_s", fb);
+    float* oc = (float*)c->buf("at_o", fb);
+    int* e = (int*)c->buf("at_e", sizeof(int) * (size_t)a.n);
+    ElemTable* t = (ElemTable*)c->buf("at_tab", sizeof(ElemTable) * tabs.size());
+    CK(cudaMemcpyAsync(x, a.x, fb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(y, a.y, fb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(z, a.z, fb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(sg, a.sigma, fb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(oc, a.occ, fb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(e, el.data(), sizeof(int) * (size_t)a.n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(t, tabs.data(), sizeof(ElemTable) * tabs.size(), cudaMemcpyHostToDevice, c->stream));
+    d.x = x; d.y = y; d.z = z; d.sig = sg; d.occ = oc; d.elem = e; d.tables = t;
+    d.n_elem = (int)tabs.size();
+    return d;
+}
+
+// Displaced, sliced and slice-sorted atoms of a group of configurations.
+struct SpecGroup {
+    int nconf = 0;
+    std::vector<int> confs;
+    std::vector<int> ns;
+    std::vector<double> z_init;
+    int S_cap = 0;
+    const float *ax = nullptr, *ay = nullptr, *aw = nullptr;
+    const int* ae = nullptr;
+    const int64_t* seg = nullptr;
+    const int* ns_d = nullptr;
+};
+
+inline float ord2f(unsigned k)
+{
+    unsigned b = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const std::vector<int>& confs,
+                         const Physics& ph)
+{
+    SpecGroup g;
+    g.confs = confs;
+    g.nconf = (int)confs.size();
+    const int64_t n = A.n, nc = g.nconf;
+    cudaStream_t st = c->stream;
+    int* dconf = (int*)c->buf("sp_conf", sizeof(int) * nc);
+    CK(cudaMemcpyAsync(dconf, confs.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+    size_t fb = sizeof(float) * (size_t)(n * nc);
+    float* xd = (float*)c->buf("sp_xd", fb);
+    float* yd = (float*)c->buf("sp_yd", fb);
+    float* zd = (float*)c->buf("sp_zd", fb);
+    launch_displace(A.x, A.y, A.z, A.sig, n, dconf, (int)nc, p.pn_seed, p.pn_dim_x, p.pn_dim_y, p.pn_dim_z, xd, yd,
+                    zd, st);
+    unsigned* zr = (unsigned*)c->buf("sp_zr", sizeof(unsigned) * 2 * nc);
+    launch_zrange(zd, n, (int)nc, zr, zr + nc, st);
+    std::vector<unsigned> zh(2 * nc);
+    CK(cudaMemcpyAsync(zh.data(), zr, sizeof(unsigned) * 2 * nc, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // slicing planes on the host, bit-identical with the device arithmetic
+    const float dz = (float)p.dz;
+    const int border = border_of(p);
+    std::vector<int> nv(nc);
+    std::vector<float> vmax(nc);
+    g.ns.resize(nc);
+    g.z_init.resize(nc);
+    int S_cap = 1;
+    for (int i = 0; i < nc; i++) {
+        float lo = ord2f(zh[i]), hi = ord2f(zh[nc + i]);
+        nv[i] = det_nplanes(lo, hi, dz);
+        vmax[i] = hi;
+        g.ns[i] = nv[i] - 1;
+        S_cap = std::max(S_cap, g.ns[i]);
+    }
+    MS_REQUIRE(S_cap <= 100000, MS_ERR_INVALID_ARG, "more than 100000 slices");
+    const int bstride = S_cap + 1;
+    std::vector<float> bounds((size_t)nc * bstride, 0.0f);
+    for (int i = 0; i < nc; i++) {
+        float lo = ord2f(zh[i]), hi = ord2f(zh[nc + i]);
+        for (int k = 0; k < nv[i]; k++) bounds[(size_t)i * bstride + k] = det_plane(k, nv[i], lo, hi, dz, border);
+        float sum = bounds[(size_t)i * bstride] + bounds[(size_t)i * bstride + 1];
+        g.z_init[i] = (double)(float)(0.5 * (double)sum);  // Slice::z_m (slice.hpp:19-22)
+    }
+    g.S_cap = S_cap;
+    float* db = (float*)c->buf("sp_bounds", sizeof(float) * bounds.size());
+    int* dnv = (int*)c->buf("sp_nv", sizeof(int) * nc);
+    float* dvmax = (float*)c->buf("sp_vmax", sizeof(float) * nc);
+    int* dns = (int*)c->buf("sp_ns", sizeof(int) * nc);
+    CK(cudaMemcpyAsync(db, bounds.data(), sizeof(float) * bounds.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dnv, nv.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dvmax, vmax.data(), sizeof(float) * nc, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dns, g.ns.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+    const int nkeys = (int)(nc * (S_cap + 1));
+    const int64_t total = n * nc;
+    MS_REQUIRE(total < (1LL << 31), MS_ERR_UNSUPPORTED, "atoms x configurations must stay below 2^31 per group");
+    unsigned* keys = (unsigned*)c->buf("sp_keys", sizeof(unsigned) * total);
+    unsigned* keys2 = (unsigned*)c->buf("sp_keys2", sizeof(unsigned) * total);
+    int* vals = (int*)c->buf("sp_vals", sizeof(int) * total);
+    int* vals2 = (int*)c->buf("sp_vals2", sizeof(int) * total);
+    unsigned* counts = (unsigned*)c->buf("sp_counts", sizeof(unsigned) * nkeys);
+    CK(cudaMemsetAsync(counts, 0, sizeof(unsigned) * nkeys, st));
+    launch_assign(zd, n, (int)nc, db, bstride, dnv, dvmax, S_cap, keys, vals, counts, st);
+    int end_bit = 1;
+    while ((1LL << end_bit) < nkeys) end_bit++;
+    size_t tmp_bytes = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, vals2, (int)total, 0, end_bit, st));
+    void* tmp = c->buf("sp_sorttmp", tmp_bytes);
+    CK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, vals2, (int)total, 0, end_bit, st));
+    int64_t* seg = (int64_t*)c->buf("sp_seg", sizeof(int64_t) * (nkeys + 1));
+    launch_scan_counts(counts, nkeys, seg, st);
+    float* ax = (float*)c->buf("sp_ax", sizeof(float) * total);
+    float* ay = (float*)c->buf("sp_ay", sizeof(float) * total);
+    float* aw = (float*)c->buf("sp_aw", sizeof(float) * total);
+    int* ae = (int*)c->buf("sp_ae", sizeof(int) * total);
+    launch_gather(keys2, vals2, total, n, S_cap, xd, yd, A.occ, A.elem, (float)ph.vr_factor, ax, ay, aw, ae, st);
+    g.ax = ax; g.ay = ay; g.aw = aw; g.ae = ae; g.seg = seg; g.ns_d = dns;
+    return g;
+}
+
+PotArgs pot_args(const ms_params& p, const Setup& s, const AtomsDev& A, const SpecGroup& g, float* V,
+                 int64_t conf_stride, int slice0, int nslice, int base)
+{
+    PotArgs a;
+    a.ax = g.ax; a.ay = g.ay; a.aw = g.aw; a.ae = g.ae; a.seg = g.seg; a.ns = g.ns_d;
+    a.S_cap = g.S_cap;
+    a.slice0 = slice0;
+    a.nslice = nslice;
+    a.V = V;
+    a.V_conf_stride = conf_stride;
+    a.V_slice_base = base;
+    a.nx = p.nx;
+    a.ny = p.ny;
+    a.dx = (float)s.gc.dx;
+    a.dy = (float)s.gc.dy;
+    a.lx = (float)p.lx;
+    a.ly = (float)p.ly;
+    a.wrap = p.pot_wrap ? 1 : 0;
+    a.elems = A.tables;
+    a.n_elem = A.n_elem;
+    return a;
+}
+
+PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const float* sV, int64_t slot_stride,
+                   const LensDev& lens)
+{
+    PassArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.psi = psi;
+    a.waves = waves;
+    a.sV = sV;
+    a.sV_slot_stride = slot_stride;
+    a.sV_slice_base = 0;
+    a.prop_x = s.prop_x;
+    a.prop_y = s.prop_y;
+    a.grid = s.gd;
+    a.lens = lens;
+    return a;
+}
+
+struct Timer {
+    ms_ctx* c;
+    int64_t l0;
+    explicit Timer(ms_ctx* cc) : c(cc), l0(kernel_launches()) { CK(cudaEventRecord(c->ev0, c->stream)); }
+    void stop()
+    {
+        CK(cudaEventRecord(c->ev1, c->stream));
+        CK(cudaEventSynchronize(c->ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->last_ms = ms;
+        c->last_launches = kernel_launches() - l0;
+        if (c->profile) c->prof_resolve();
+    }
+};
+
+// free device memory budget for the potential store
+size_t free_budget()
+{
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    return (size_t)(fr * 0.6);
+}
+
+void copy_out(ms_ctx* c, float* dst, const float* src, int64_t n, int on_dev)
+{
+    CK(cudaMemcpyAsync(dst, src, sizeof(float) * n, on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       c->stream));
+}
+
+int estimate_slices(const ms_params& p, const ms_atoms& a)
+{
+    float lo = a.z[0], hi = a.z[0], smax = 0.f;
+    for (int64_t i = 0; i < a.n; i++) {
+        lo = std::min(lo, a.z[i]);
+        hi = std::max(hi, a.z[i]);
+        smax = std::max(smax, a.sigma[i]);
+    }
+    return (int)((hi - lo + 12.0f * smax) / (float)p.dz) + 3;
+}
+
+}  // namespace
+
+void ctx_activate(ms_ctx* c)
+{
+    CK(cudaSetDevice(c->device));
+    if (!c->constants_ready) {
+        upload_constants(c->stream);
+        c->constants_ready = true;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// HRTEM / ED (ED_HRTEM, single_simulator.cuh:11-126) and CBED (CBED_CBEI, :128-206)
+// ---------------------------------------------------------------------------
+void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed)
+{
+    validate_params(p);
+    validate_atoms(p, &a);
+    MS_REQUIRE(out != nullptr, MS_ERR_INVALID_ARG, "output is NULL");
+    const bool kspace = force_cbed || p.simulation_type != MS_SIM_HRTEM;
+    const bool full = p.data_record == MS_RECORD_WAVE;
+    MS_REQUIRE(full ? (out->image_real && out->image_imag) : (out->image_intensity != nullptr), MS_ERR_INVALID_ARG,
+               "output buffers for the requested data_record are NULL");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    Timer tm(c);
+    Setup s = make_setup(c, p);
+    const int64_t N = s.N;
+    AtomsDev A = upload_atoms(c, p, a);
+    ConfSet cs = conf_set(p);
+    const int iw = force_cbed ? (p.iw_type > 0 ? p.iw_type : MS_IW_CONVERGENT) : iw_of(p);
+    LensDev cond = lens_dev(lens_coef(p.cond_lens, s.ph.lambda, 0.0));
+    LensDev obj = lens_dev(lens_coef(p.obj_lens, s.ph.lambda, 0.0));
+
+    // configurations per group: potential store + waves must fit the memory budget
+    int S_est = estimate_slices(p, a);
+    size_t per_conf = (size_t)S_est * N * 4 + (size_t)N * 8 * 2 + (size_t)N * 4 + (size_t)a.n * 40;
+    int gsize = (int)std::max<size_t>(1, std::min<size_t>(cs.confs.size(), free_budget() / per_conf));
+
+    double* acc = (double*)c->buf("acc0", sizeof(double) * N);
+    double* acc_im = full ? (double*)c->buf("acc1", sizeof(double) * N) : nullptr;
+    bool first = true;
+    int ns_first = 0;
+    for (size_t g0 = 0; g0 < cs.confs.size(); g0 += gsize) {
+        std::vector<int> confs(cs.confs.begin() + g0, cs.confs.begin() + std::min(cs.confs.size(), g0 + gsize));
+        SpecGroup g = build_specimen(c, p, A, confs, s.ph);
+        if (g0 == 0) ns_first = g.ns[0];
+        const int nw = g.nconf;
+        const int64_t slot = (int64_t)g.S_cap * N;
+        float* sV = (float*)c->buf("sV", sizeof(float) * slot * nw);
+        run_potential(c, pot_args(p, s, A, g, sV, slot, 0, g.S_cap, 0), nw, st);
+        std::vector<WaveInfo> wv(nw);
+        for (int i = 0; i < nw; i++) {
+            wv[i].px = p.iw_x;
+            wv[i].py = p.iw_y;
+            wv[i].cc10 = gate_coef(-kPi * (p.cond_lens.c10 + g.z_init[i]) * s.ph.lambda);
+            wv[i].conf_slot = i;
+            wv[i].n_slices = g.ns[i];
+            wv[i].weight = (float)cs.weight;
+            wv[i].pos = 0;
+        }
+        WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * nw);
+        CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nw, cudaMemcpyHostToDevice, st));
+        float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * nw);
+        PassArgs pa = pass_args(s, psi, dwv, sV, slot, cond);
+        if (iw == MS_IW_CONVERGENT) {
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_PROBE_INV, pa, nw, p.nx, st);
+        }
+        const int S_max = *std::max_element(g.ns.begin(), g.ns.end());
+        for (int sl = 0; sl < S_max; sl++) {
+            pa.slice = sl;
+            pa.tw = s.tw_x;
+            run_row(c, p.nx, (sl == 0 && iw == MS_IW_PLANE) ? ROW_T_FWD : ROW_INV_T_FWD, pa, nw, p.ny, st);
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_STEP, pa, nw, p.nx, st);
+        }
+        if (!kspace) {
+            // OL_modulation -> CTF_TEM (wave_function.cuh:96-110, lens_modulation.cuh:78-89)
+            pa.lens = obj;
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_CTF_INV, pa, nw, p.nx, st);
+            pa.tw = s.tw_x;
+            if (full) {
+                float2* aux = (float2*)c->buf("aux", sizeof(float2) * N * nw);
+                pa.aux = aux;
+                run_row(c, p.nx, ROW_INV_STORE, pa, nw, p.ny, st);
+                launch_acc_cplx(aux, nw, dwv, N, acc, acc_im, first, st);
+            } else {
+                float* img = (float*)c->buf("img_w", sizeof(float) * N * nw);
+                pa.out_real = img;
+                run_row(c, p.nx, ROW_INV_ABS2, pa, nw, p.ny, st);
+                launch_acc_real(img, nw, N, acc, first, st);
+            }
+        } else {
+            if (full) launch_acc_cplx(psi, nw, dwv, N, acc, acc_im, first, st);
+            else launch_acc_abs2(psi, nw, dwv, N, acc, first, st);
+        }
+        first = false;
+        CK(cudaStreamSynchronize(st));  // host wave table reused by the next group
+    }
+    float* o0 = (float*)c->buf("out0", sizeof(float) * N);
+    launch_emit(acc, p.nx, p.ny, kspace ? 1 : 0, o0, st);
+    if (full) {
+        copy_out(c, out->image_real, o0, N, out->on_device);
+        float* o1 = (float*)c->buf("out1", sizeof(float) * N);
+        launch_emit(acc_im, p.nx, p.ny, kspace ? 1 : 0, o1, st);
+        copy_out(c, out->image_imag, o1, N, out->on_device);
+    } else {
+        copy_out(c, out->image_intensity, o0, N, out->on_device);
+    }
+    tm.stop();
+    out->row = p.ny;
+    out->col = p.nx;
+    out->n_slices = ns_first;
+    out->interval_x = p.lx / p.nx;
+    out->interval_y = p.ly / p.ny;
+    out->total_intensity = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// STEM (run_STEM_tile_simu, scan_simulator.cuh:11-113; plain form run_STEM_general_simu, :115-183)
+// ---------------------------------------------------------------------------
+namespace {
+int choose_batch(const ms_params& p, int npos, int64_t N)
+{
+    if (p.exec_mode == MS_EXEC_PLAIN) return 1;
+    if (p.probe_batch > 0) return std::min(p.probe_batch, npos);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    int64_t cap = (int64_t)(fr * 0.25 / (double)(N * 8));
+    int b = (int)std::min<int64_t>(256, std::max<int64_t>(1, cap));
+    return std::min(b, npos);
+}
+}  // namespace
+
+void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
+{
+    validate_params(p);
+    validate_atoms(p, &a);
+    MS_REQUIRE(p.simulation_type == MS_SIM_STEM, MS_ERR_INVALID_ARG, "simulation_type must be STEM");
+    MS_REQUIRE(out != nullptr && out->stem_intensity != nullptr, MS_ERR_INVALID_ARG, "stem_intensity is NULL");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    Timer tm(c);
+    Setup s = make_setup(c, p);
+    const int64_t N = s.N;
+    AtomsDev A = upload_atoms(c, p, a);
+    ConfSet cs = conf_set(p);
+    LensDev cond = lens_dev(lens_coef(p.cond_lens, s.ph.lambda, 0.0));
+    const int npos = p.scan_nx * p.scan_ny, ndet = p.n_det;
+    const bool plain = p.exec_mode == MS_EXEC_PLAIN;
+    std::vector<float> thr(2 * ndet);
+    for (int d = 0; d < ndet; d++) {
+        thr[d] = g2_threshold(p.det_inner[d], s.ph.lambda);
+        thr[ndet + d] = g2_threshold(p.det_outer[d], s.ph.lambda);
+    }
+    float* dthr = (float*)c->buf("det_thr", sizeof(float) * 2 * ndet);
+    CK(cudaMemcpyAsync(dthr, thr.data(), sizeof(float) * 2 * ndet, cudaMemcpyHostToDevice, st));
+    double* img = (double*)c->buf("stem_acc", sizeof(double) * ndet * npos);
+    CK(cudaMemsetAsync(img, 0, sizeof(double) * ndet * npos, st));
+    const int B = choose_batch(p, npos, N);
+    const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
+    double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
+    double* Iw = (double*)c->buf("det_I", sizeof(double) * B * ndet);
+    std::vector<WaveInfo> wv((size_t)B);
+    std::vector<double> Ih((size_t)B * ndet);
+    for (int conf : cs.confs) {
+        SpecGroup g = build_specimen(c, p, A, std::vector<int>{conf}, s.ph);
+        const int S = g.ns[0];
+        const double cc10 = gate_coef(-kPi * (p.cond_lens.c10 + g.z_init[0]) * s.ph.lambda);
+        float* sV;
+        int64_t slot = (int64_t)S * N;
+        if (!plain) {
+            sV = (float*)c->buf("sV", sizeof(float) * slot);
+            run_potential(c, pot_args(p, s, A, g, sV, slot, 0, S, 0), 1, st);
+        } else {
+            sV = (float*)c->buf("sV1", sizeof(float) * N);
+        }
+        for (int start = 0; start < npos; start += B) {
+            const int nb = std::min(B, npos - start);
+            for (int i = 0; i < nb; i++) {
+                int ip = start + i, ix = ip % p.scan_nx, iy = ip / p.scan_nx;
+                wv[i].px = p.scan_x0 + ix * p.scan_dx;
+                wv[i].py = p.scan_y0 + iy * p.scan_dy;
+                wv[i].cc10 = cc10;
+                wv[i].conf_slot = 0;
+                wv[i].n_slices = S;
+                wv[i].weight = (float)cs.weight;
+                wv[i].pos = ip;
+            }
+            WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * B);
+            CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nb, cudaMemcpyHostToDevice, st));
+            float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * B);
+            PassArgs pa = pass_args(s, psi, dwv, sV, plain ? 0 : slot, cond);
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_PROBE_INV, pa, nb, p.nx, st);
+            for (int sl = 0; sl < S; sl++) {
+                pa.slice = sl;
+                if (plain) {
+                    // the reference's general scan regenerates the slice potential for every probe
+                    // (transmit -> generate_potential_single_slice, transmission_function.cuh:107-111)
+                    run_potential(c, pot_args(p, s, A, g, sV, 0, sl, 1, sl), 1, st);
+                    pa.sV_slice_base = sl;
+                }
+                pa.tw = s.tw_x;
+                run_row(c, p.nx, ROW_INV_T_FWD, pa, nb, p.ny, st);
+                pa.tw = s.tw_y;
+                run_col(c, p.ny, COL_STEP, pa, nb, p.nx, st);
+            }
+            launch_detect(psi, nb, p.nx, p.ny, s.gd.dgx_f, s.gd.dgy_f, dthr, dthr + ndet, ndet, partial, nblk, st);
+            launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw, img, npos, 1, st);
+            if (plain) {
+                // integrated_intensity: a blocking read of the probe's detector sums (wave_function.cuh:135-146)
+                CK(cudaMemcpyAsync(Ih.data(), Iw, sizeof(double) * nb * ndet, cudaMemcpyDeviceToHost, st));
+            }
+            CK(cudaStreamSynchronize(st));  // the host wave table is refilled by the next batch
+        }
+    }
+    float* o = (float*)c->buf("stem_out", sizeof(float) * ndet * npos);
+    launch_d2f(img, (int64_t)ndet * npos, o, st);
+    copy_out(c, out->stem_intensity, o, (int64_t)ndet * npos, out->on_device);
+    tm.stop();
+    out->row = p.scan_ny;
+    out->col = p.scan_nx;
+    out->interval_x = p.scan_dx;
+    out->interval_y = p.scan_dy;
+    out->n_slices = 0;
+    // total_intensity: vacuum exit intensity sum_k N^2 A(k) (the reference's blank intensity
+    // table, scan_simulator.cuh:34); probes have |Psi0(k)| in {0,1}
+    {
+        LensCoef L = lens_coef(p.cond_lens, s.ph.lambda, 0.0);
+        double tot = 0.0;
+        for (int iy = 0; iy < p.ny; iy++)
+            for (int ix = 0; ix < p.nx; ix++) {
+                float g2 = det_g2(ix, iy, p.nx, p.ny, s.gd.dgx_f, s.gd.dgy_f);
+                if (L.g2min <= g2 && g2 < L.g2max) tot += 1.0;
+            }
+        out->total_intensity = tot * (double)N * (double)N;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// thickness series (run_thickness_simu, thickness_simulator.cuh:11-85)
+// ---------------------------------------------------------------------------
+void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
+{
+    validate_params(p);
+    validate_atoms(p, &a);
+    MS_REQUIRE(out != nullptr && out->thickness_frames != nullptr, MS_ERR_INVALID_ARG, "thickness_frames is NULL");
+    MS_REQUIRE(p.thick_det >= 0 && p.thick_det < p.n_det, MS_ERR_INVALID_ARG, "thick_det must name a detector");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    Timer tm(c);
+    Setup s = make_setup(c, p);
+    const int64_t N = s.N;
+    AtomsDev A = upload_atoms(c, p, a);
+    ConfSet cs = conf_set(p);
+    LensDev cond = lens_dev(lens_coef(p.cond_lens, s.ph.lambda, 0.0));
+    const int iw = iw_of(p);
+    // frames follow the static specimen's slices (thickness_simulator.cuh:22-25)
+    std::vector<int> sl0(a.n);
+    int nf = host_slices(p, a.z, a.n, nullptr, nullptr);
+    MS_REQUIRE((int64_t)nf * N <= out->thickness_capacity, MS_ERR_INVALID_ARG,
+               "thickness_frames holds fewer than n_slices*ny*nx floats");
+    float* frames = (float*)c->buf("frames", sizeof(float) * N * nf);
+    CK(cudaMemsetAsync(frames, 0, sizeof(float) * N * nf, st));
+    float* dthr = nullptr;
+    (void)dthr;
+    const float g2in = g2_threshold(p.det_inner[p.thick_det], s.ph.lambda);
+    const float g2out = g2_threshold(p.det_outer[p.thick_det], s.ph.lambda);
+    for (int conf : cs.confs) {
+        SpecGroup g = build_specimen(c, p, A, std::vector<int>{conf}, s.ph);
+        const int S = g.ns[0];
+        const int64_t slot = (int64_t)S * N;
+        float* sV = (float*)c->buf("sV", sizeof(float) * slot);
+        run_potential(c, pot_args(p, s, A, g, sV, slot, 0, S, 0), 1, st);
+        WaveInfo wv;
+        wv.px = p.iw_x;
+        wv.py = p.iw_y;
+        wv.cc10 = gate_coef(-kPi * (p.cond_lens.c10 + g.z_init[0]) * s.ph.lambda);
+        wv.conf_slot = 0;
+        wv.n_slices = S;
+        wv.weight = (float)cs.weight;
+        wv.pos = 0;
+        WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo));
+        CK(cudaMemcpyAsync(dwv, &wv, sizeof(WaveInfo), cudaMemcpyHostToDevice, st));
+        float2* psi = (float2*)c->buf("psi", sizeof(float2) * N);
+        float2* aux = (float2*)c->buf("aux", sizeof(float2) * N);
+        PassArgs pa = pass_args(s, psi, dwv, sV, slot, cond);
+        pa.aux = aux;
+        pa.filt_g2in = g2in;
+        pa.filt_g2out = g2out;
+        if (iw == MS_IW_CONVERGENT) {
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_PROBE_INV, pa, 1, p.nx, st);
+        }
+        for (int sl = 0; sl < nf; sl++) {
+            pa.slice = sl;
+            pa.flags = PF_VACUUM_BEYOND;
+            pa.tw = s.tw_x;
+            run_row(c, p.nx, (sl == 0 && iw == MS_IW_PLANE) ? ROW_T_FWD : ROW_INV_T_FWD, pa, 1, p.ny, st);
+            pa.flags = PF_VACUUM_BEYOND | PF_PROP_ALWAYS | PF_FILTER_AUX;
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_STEP, pa, 1, p.nx, st);
+            // filtered branch: IFFT2 of the annulus-masked spectrum, |.|^2 into frame sl (Filter_wave,
+            // device_kernels.cuh:389-410, wave_filter, wave_function.cuh:163-174)
+            PassArgs pb = pa;
+            pb.psi = aux;
+            pb.aux = aux;
+            pb.flags = 0;
+            run_col(c, p.ny, COL_INV, pb, 1, p.nx, st);
+            pb.flags = PF_FILTER_AUX | PF_ACCUMULATE;
+            pb.out_real = frames + (int64_t)sl * N;
+            pb.tw = s.tw_x;
+            run_row(c, p.nx, ROW_INV_ABS2, pb, 1, p.ny, st);
+        }
+        CK(cudaStreamSynchronize(st));
+    }
+    copy_out(c, out->thickness_frames, frames, (int64_t)nf * N, out->on_device);
+    tm.stop();
+    out->row = p.ny;
+    out->col = p.nx;
+    out->n_slices = nf;
+    out->interval_x = p.lx / p.nx;
+    out->interval_y = p.ly / p.ny;
+}
+
+// ---------------------------------------------------------------------------
+// projected potentials of one configuration
+// ---------------------------------------------------------------------------
+void sim_potential(ms_ctx* c, const ms_params& p, const ms_atoms& a, int conf, float* V, int64_t cap, int on_dev,
+                   int* n_slices)
+{
+    validate_params(p);
+    validate_atoms(p, &a);
+    MS_REQUIRE(conf >= 0, MS_ERR_INVALID_ARG, "conf must be >= 0");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    Timer tm(c);
+    Setup s = make_setup(c, p);
+    AtomsDev A = upload_atoms(c, p, a);
+    SpecGroup g = build_specimen(c, p, A, std::vector<int>{conf}, s.ph);
+    const int S = g.ns[0];
+    if (n_slices) *n_slices = S;
+    if (V) {
+        MS_REQUIRE((int64_t)S * s.N <= cap, MS_ERR_INVALID_ARG, "V_out holds fewer than n_slices*ny*nx floats");
+        int64_t slot = (int64_t)S * s.N;
+        float* sV = (float*)c->buf("sV", sizeof(float) * slot);
+        run_potential(c, pot_args(p, s, A, g, sV, slot, 0, S, 0), 1, st);
+        copy_out(c, V, sV, slot, on_dev);
+    }
+    tm.stop();
+}
+
+// ---------------------------------------------------------------------------
+// STEM on caller potentials (wave_modulation_batch, wave_function.cuh:74-87)
+// ---------------------------------------------------------------------------
+void sim_stem_forward_potential(ms_ctx* c, const ms_params& p, const float* V, int S, int on_dev, double z_init,
+                                const double* xy, int np, float* I)
+{
+    validate_params(p);
+    MS_REQUIRE(V && xy && I && S >= 1 && np >= 1 && p.n_det >= 1, MS_ERR_INVALID_ARG, "bad arguments");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    Timer tm(c);
+    Setup s = make_setup(c, p);
+    const int64_t N = s.N, slot = (int64_t)S * N;
+    LensDev cond = lens_dev(lens_coef(p.cond_lens, s.ph.lambda, 0.0));
+    const float* sV = V;
+    if (!on_dev) {
+        float* d = (float*)c->buf("sV", sizeof(float) * slot);
+        CK(cudaMemcpyAsync(d, V, sizeof(float) * slot, cudaMemcpyHostToDevice, st));
+        sV = d;
+    }
+    const int ndet = p.n_det;
+    std::vector<float> thr(2 * ndet);
+    for (int d = 0; d < ndet; d++) {
+        thr[d] = g2_threshold(p.det_inner[d], s.ph.lambda);
+        thr[ndet + d] = g2_threshold(p.det_outer[d], s.ph.lambda);
+    }
+    float* dthr = (float*)c->buf("det_thr", sizeof(float) * 2 * ndet);
+    CK(cudaMemcpyAsync(dthr, thr.data(), sizeof(float) * 2 * ndet, cudaMemcpyHostToDevice, st));
+    const int B = std::min(np, p.probe_batch > 0 ? p.probe_batch : 256);
+    const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
+    double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
+    double* Iw = (double*)c->buf("det_I_all", sizeof(double) * np * ndet);
+    const double cc10 = gate_coef(-kPi * (p.cond_lens.c10 + z_init) * s.ph.lambda);
+    std::vector<WaveInfo> wv((size_t)B);
+    for (int start = 0; start < np; start += B) {
+        const int nb = std::min(B, np - start);
+        for (int i = 0; i < nb; i++) {
+            wv[i].px = xy[2 * (start + i)];
+            wv[i].py = xy[2 * (start + i) + 1];
+            wv[i].cc10 = cc10;
+            wv[i].conf_slot = 0;
+            wv[i].n_slices = S;
+            wv[i].weight = 1.0f;
+            wv[i].pos = start + i;
+        }
+        WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * B);
+        CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nb, cudaMemcpyHostToDevice, st));
+        float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * B);
+        PassArgs pa = pass_args(s, psi, dwv, sV, slot, cond);
+        pa.tw = s.tw_y;
+        run_col(c, p.ny, COL_PROBE_INV, pa, nb, p.nx, st);
+        for (int sl = 0; sl < S; sl++) {
+            pa.slice = sl;
+            pa.tw = s.tw_x;
+            run_row(c, p.nx, ROW_INV_T_FWD, pa, nb, p.ny, st);
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_STEP, pa, nb, p.nx, st);
+        }
+        launch_detect(psi, nb, p.nx, p.ny, s.gd.dgx_f, s.gd.dgy_f, dthr, dthr + ndet, ndet, partial, nblk, st);
+        launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw + (int64_t)start * ndet, nullptr, 0, 0, st);
+        CK(cudaStreamSynchronize(st));
+    }
+    float* o = (float*)c->buf("stem_out", sizeof(float) * np * ndet);
+    launch_d2f(Iw, (int64_t)np * ndet, o, st);
+    CK(cudaMemcpyAsync(I, o, sizeof(float) * np * ndet, cudaMemcpyDeviceToHost, st));
+    tm.stop();
+}
+
+void sim_stem_backward(ms_ctx*, const ms_params&, const float*, int, int, double, const double*, int, const float*,
+                       double*, float*, double*, double*)
+{
+    throw MsError(MS_ERR_UNSUPPORTED, "the adjoint is not built into this library yet");
+}
+
+void sim_many(ms_ctx*, int, const ms_params*, const ms_atoms*, ms_output*, double*)
+{
+    throw MsError(MS_ERR_UNSUPPORTED, "uneven batches are not built into this library yet");
+}
+
+}  // namespace msb

@@ -1,0 +1,118 @@
+// FP32 complex FFT building blocks for the fused slice passes.
+//
+// An N-point transform is computed by a "team" of G threads, each holding
+// E = N/G points in registers, as a two-level Cooley-Tukey factorisation
+// N = E x G:
+//   1. each thread g takes x[g + G j] (j < E) and runs an E-point DFT in
+//      registers (radix-2 decimation in frequency, constant twiddles from
+//      __constant__ memory, fully unrolled);
+//   2. the E outputs are multiplied by the inter-level twiddles W_N^(g k1)
+//      (a shared-memory table laid out [k1][g] so a team reads it without
+//      bank conflicts);
+//   3. one transpose through shared memory (padded rows) hands every thread
+//      the G values of E/G columns k1, and a G-point register DFT finishes
+//      each.
+// The result is X[g + G j'] in thread g, i.e. the same distribution as the
+// input, so an inverse transform, a pointwise multiply and a forward
+// transform chain in registers with no data movement.  Forward transforms
+// use exp(-2 pi i jk/N) and are unnormalised, like CUFFT_FORWARD.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft_layout.hpp"
+
+namespace msb {
+
+// W_64^m = exp(-2 pi i m / 64), rounded from FP64 on the host (upload_constants).
+// Defined here: only kernels.cu includes this header.
+__constant__ float2 c_tw64[64];
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// Multiply by W_64^m (DIR < 0) or its conjugate (DIR > 0); m is a compile-time
+// constant once the callers are unrolled.
+template <int DIR>
+__device__ __forceinline__ float2 tw_apply(float2 d, int m)
+{
+    if (m == 0) return d;
+    if (m == 16) return DIR < 0 ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);
+    float2 w = c_tw64[m];
+    return DIR < 0 ? cmul(d, w) : cmulc(d, w);
+}
+
+template <int E>
+__host__ __device__ constexpr int brev(int k)
+{
+    int r = 0;
+    for (int b = 1; b < E; b <<= 1) {
+        r = (r << 1) | (k & 1);
+        k >>= 1;
+    }
+    return r;
+}
+
+// In-register E-point DFT, E a power of two <= 64.  Output in bit-reversed
+// order: after the call a[brev<E>(k)] holds X[k].
+template <int E, int DIR>
+__device__ __forceinline__ void dft_reg(float2 (&a)[E])
+{
+#pragma unroll
+    for (int len = E; len >= 2; len >>= 1) {
+        const int half = len >> 1;
+#pragma unroll
+        for (int base = 0; base < E; base += len) {
+#pragma unroll
+            for (int j = 0; j < half; j++) {
+                float2 u = a[base + j], v = a[base + j + half];
+                a[base + j] = cadd(u, v);
+                a[base + j + half] = tw_apply<DIR>(csub(u, v), j * (64 / len));
+            }
+        }
+    }
+}
+
+// Team transform.  On entry v[j] = x[g + G j]; on exit v[j] = X[g + G j].
+// `tw` is the shared table W_N^(g k1) at tw[k1 * G + g].  `scr(k1, g)` returns
+// the shared-memory slot for the transpose; `sync()` orders the team's shared
+// accesses (a warp barrier when the team is inside one warp, a block barrier
+// otherwise).
+template <int N, int G, int DIR, class Scr, class Sync>
+__device__ __forceinline__ void team_fft(float2 (&v)[N / G], int g, const float2* __restrict__ tw, Scr scr,
+                                         Sync sync)
+{
+    constexpr int E = N / G;
+    static_assert(E >= G && E % G == 0, "team layout needs E >= G");
+    dft_reg<E, DIR>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < E; k1++) {
+        float2 w = tw[k1 * G + g];
+        v[brev<E>(k1)] = DIR < 0 ? cmul(v[brev<E>(k1)], w) : cmulc(v[brev<E>(k1)], w);
+    }
+    sync();
+#pragma unroll
+    for (int k1 = 0; k1 < E; k1++) *scr(k1, g) = v[brev<E>(k1)];
+    sync();
+    constexpr int M = E / G;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        float2 u[G];
+#pragma unroll
+        for (int q = 0; q < G; q++) u[q] = *scr(g + G * m, q);
+        dft_reg<G, DIR>(u);
+#pragma unroll
+        for (int k2 = 0; k2 < G; k2++) v[m + M * k2] = u[brev<G>(k2)];
+    }
+}
+
+}  // namespace msb

@@ -1,0 +1,808 @@
+// Kernels of the multislice engine.
+//
+// Per slice the wave batch makes two passes through memory:
+//   row pass    : inverse row FFT -> transmission t_s = exp(i sigma V_s) -> forward row FFT
+//   column pass : forward column FFT -> Fresnel propagator P(k) -> inverse column FFT
+// which together equal the reference's transmit (forward cuFFT with the
+// exp(iV) load callback, transmission_function.cuh:107-119) and propagate
+// (inverse cuFFT with the P load callback, propagation_function.cuh:41-48).
+// The probe is generated inside the first column pass, the CTF inside the
+// HRTEM column pass and the detector sums in a read-only post pass.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <atomic>
+#include <cfloat>
+
+#include "detmath.cuh"
+#include "fft.cuh"
+#include "kernels.cuh"
+
+namespace msb {
+
+static std::atomic<int64_t> g_launches{0};
+int64_t kernel_launches() { return g_launches.load(); }
+void reset_kernel_launches() { g_launches.store(0); }
+static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+static void check_launch(const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw MsError(MS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void upload_constants(cudaStream_t st)
+{
+    float2 t[64];
+    for (int m = 0; m < 64; m++) {
+        double a = -2.0 * 3.14159265358979323846264338327950288 * m / 64.0;
+        t[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_tw64, t, sizeof(t), 0, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) throw MsError(MS_ERR_CUDA, std::string("constant upload: ") + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// lens phase (coherent_phase_shift, basic_functions_dev.cuh:215-234) in FP64
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double chi_d(const LensDev& L, double cc10, double gx, double gy)
+{
+    double g2 = gx * gx + gy * gy, g4 = g2 * g2, g6 = g4 * g2;
+    double chi = cc10 * g2 + L.cc30 * g4 + L.cc50 * g6;
+    if (L.phi_req) {
+        double g = sqrt(g2), g3 = g2 * g, g5 = g4 * g;
+        double ph = atan2(gy, gx);
+        if (fabs(ph) > 1e-5) chi += L.m * ph;
+        chi += L.cc12 * g2 * sin(2 * (ph - L.p12));
+        chi += L.cc21 * g3 * sin(ph - L.p21) + L.cc23 * g3 * sin(3 * (ph - L.p23));
+        chi += L.cc32 * g4 * sin(2 * (ph - L.p32)) + L.cc34 * g4 * sin(4 * (ph - L.p34));
+        chi += L.cc41 * g5 * sin(ph - L.p41) + L.cc43 * g5 * sin(3 * (ph - L.p43)) + L.cc45 * g5 * sin(5 * (ph - L.p45));
+        chi += L.cc52 * g6 * sin(2 * (ph - L.p52)) + L.cc54 * g6 * sin(4 * (ph - L.p54)) + L.cc56 * g6 * sin(6 * (ph - L.p56));
+    }
+    return chi;
+}
+
+// exp(i ph) for a phase formed in FP64: reduced modulo 2 pi in FP64, then FP32 sincos.
+__device__ __forceinline__ float2 expi_d(double ph)
+{
+    const double two_pi = 6.283185307179586476925286766559;
+    double r = ph - two_pi * rint(ph * (1.0 / two_pi));
+    float s, c;
+    sincosf((float)r, &s, &c);
+    return make_float2(c, s);
+}
+
+__device__ __forceinline__ double freq_d(int i, int n, double dg) { return (double)((i < n / 2) ? i : i - n) * dg; }
+
+// ---------------------------------------------------------------------------
+// row pass
+// ---------------------------------------------------------------------------
+template <int N, int OP>
+__global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E;
+    extern __shared__ float2 smem[];
+    const int ny = a.grid.ny;
+    const int blocks_per_wave = ny / L::ROWS;
+    const int b = blockIdx.x / blocks_per_wave;
+    const int team = threadIdx.x / G, g = threadIdx.x % G;
+    const int r = (blockIdx.x % blocks_per_wave) * L::ROWS + team;
+    const WaveInfo wi = a.waves[b];
+    const bool beyond = a.slice >= wi.n_slices;
+    if ((OP == ROW_T_FWD || OP == ROW_INV_T_FWD) && beyond && !(a.flags & PF_VACUUM_BEYOND)) return;
+
+    float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = a.tw[i];
+    __syncthreads();
+    float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncwarp(); };
+
+    const size_t row_off = ((size_t)b * ny + r) * N;
+    float2 v[E];
+    if (OP == ROW_T_FWD) {
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = make_float2(1.0f, 0.0f);
+    } else {
+        const float2* src = (OP == ROW_INV_ABS2 && (a.flags & PF_FILTER_AUX)) ? a.aux : a.psi;
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = src[row_off + g + G * j];
+        team_fft<N, G, +1>(v, g, tw, scr, sync);
+    }
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD) {
+        if (!beyond) {
+            const float* vr = a.sV + (size_t)wi.conf_slot * a.sV_slot_stride + ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
+#pragma unroll
+            for (int j = 0; j < E; j++) {
+                float s, c;
+                sincosf(__ldg(vr + g + G * j), &s, &c);
+                v[j] = cmul(v[j], make_float2(c, s));
+            }
+        }
+        team_fft<N, G, -1>(v, g, tw, scr, sync);
+#pragma unroll
+        for (int j = 0; j < E; j++) a.psi[row_off + g + G * j] = v[j];
+    } else if (OP == ROW_INV_ABS2) {
+        float* o = a.out_real + ((a.flags & PF_FILTER_AUX) ? (size_t)r * N : row_off);
+        const float w = wi.weight;
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            float i2 = w * (v[j].x * v[j].x + v[j].y * v[j].y);
+            if (a.flags & PF_ACCUMULATE) o[g + G * j] += i2;
+            else o[g + G * j] = i2;
+        }
+    } else if (OP == ROW_INV_STORE) {
+#pragma unroll
+        for (int j = 0; j < E; j++) a.aux[row_off + g + G * j] = v[j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// column pass
+// ---------------------------------------------------------------------------
+template <int N, int OP>
+__global__ void __launch_bounds__(FftLayout<N>::COL_THREADS) k_col(PassArgs a)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E, TC = L::TC;
+    extern __shared__ float2 smem[];
+    const int nx = a.grid.nx;
+    const int tiles = nx / TC;
+    const int b = blockIdx.x / tiles;
+    const int col0 = (blockIdx.x % tiles) * TC;
+    const int c = threadIdx.x % TC, g = threadIdx.x / TC;
+    const int col = col0 + c;
+    const WaveInfo wi = a.waves[b];
+    bool final_step = false;
+    if (OP == COL_STEP) {
+        if (a.slice >= wi.n_slices && !(a.flags & PF_VACUUM_BEYOND)) return;
+        final_step = (a.slice == wi.n_slices - 1) && !(a.flags & PF_PROP_ALWAYS);
+    }
+
+    float2* tw = smem + TC * L::SCR_STRIDE_COL;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = a.tw[i];
+    __syncthreads();
+    float2* scr_base = smem + c * L::SCR_STRIDE_COL;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncthreads(); };
+
+    float2* base = a.psi + (size_t)b * N * nx;
+    float2 v[E];
+    if constexpr (OP == COL_PROBE_INV) {
+        // Generate_probe / Generate_multi_probe (device_kernels.cuh:363-444): aperture mask on the
+        // float frequency, phase chi + x gx + y gy formed in FP64.
+        const double gx = freq_d(col, nx, a.grid.dgx);
+        const double xf = -6.283185307179586476925 * wi.px, yf = -6.283185307179586476925 * wi.py;
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int k = g + G * j;
+            float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+            if (a.lens.g2min <= g2 && g2 < a.lens.g2max) {
+                double gy = freq_d(k, N, a.grid.dgy);
+                v[j] = expi_d(chi_d(a.lens, wi.cc10, gx, gy) + xf * gx + yf * gy);
+            } else {
+                v[j] = make_float2(0.0f, 0.0f);
+            }
+        }
+        team_fft<N, G, +1>(v, g, tw, scr, sync);
+#pragma unroll
+        for (int j = 0; j < E; j++) base[(size_t)(g + G * j) * nx + col] = v[j];
+        return;
+    } else {
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j] = base[(size_t)(g + G * j) * nx + col];
+
+    if (OP == COL_STEP) {
+        team_fft<N, G, -1>(v, g, tw, scr, sync);
+        if (final_step) {
+#pragma unroll
+            for (int j = 0; j < E; j++) base[(size_t)(g + G * j) * nx + col] = v[j];
+            return;
+        }
+        // P(k) = (1/N) bwl(g^2) exp(i w |g - g0|^2), separable phase (gen_propagator_kernel,
+        // device_kernels.cuh:215-234)
+        const float2 px = __ldg(a.prop_x + col);
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int k = g + G * j;
+            float amp = a.grid.inv_n;
+            float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+            if (a.grid.bwl) amp = amp / (1.0f + expf(a.grid.alpha_f * (g2 - a.grid.gl2_f)));
+            float2 pr = cmul(px, __ldg(a.prop_y + k));
+            v[j] = cmul(v[j], cscale(pr, amp));
+            if (a.flags & PF_FILTER_AUX) {
+                float2* ab = a.aux + (size_t)b * N * nx;
+                bool in = (a.filt_g2in <= g2 && g2 <= a.filt_g2out);
+                ab[(size_t)k * nx + col] = in ? v[j] : make_float2(0.0f, 0.0f);
+            }
+        }
+        team_fft<N, G, +1>(v, g, tw, scr, sync);
+    } else if (OP == COL_CTF_INV) {
+        // apply_CTF_kernel (device_kernels.cuh:445-468)
+        const double gx = freq_d(col, nx, a.grid.dgx);
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int k = g + G * j;
+            float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+            if (a.lens.g2min <= g2 && g2 < a.lens.g2max) {
+                double gy = freq_d(k, N, a.grid.dgy);
+                v[j] = cmul(v[j], expi_d(chi_d(a.lens, a.lens.cc10, gx, gy)));
+            } else {
+                v[j] = make_float2(0.0f, 0.0f);
+            }
+        }
+        team_fft<N, G, +1>(v, g, tw, scr, sync);
+    } else if (OP == COL_INV) {
+        team_fft<N, G, +1>(v, g, tw, scr, sync);
+    }
+#pragma unroll
+    for (int j = 0; j < E; j++) base[(size_t)(g + G * j) * nx + col] = v[j];
+    }
+}
+
+template <int N>
+static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st)
+{
+    using L = FftLayout<N>;
+    dim3 grid((unsigned)(nwaves * (ny / L::ROWS))), block(L::ROW_THREADS);
+    size_t sm = L::ROW_SMEM;
+    switch (op) {
+    case ROW_T_FWD:
+        cudaFuncSetAttribute(k_row<N, ROW_T_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row<N, ROW_T_FWD><<<grid, block, sm, st>>>(a);
+        break;
+    case ROW_INV_T_FWD:
+        cudaFuncSetAttribute(k_row<N, ROW_INV_T_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row<N, ROW_INV_T_FWD><<<grid, block, sm, st>>>(a);
+        break;
+    case ROW_INV_ABS2:
+        cudaFuncSetAttribute(k_row<N, ROW_INV_ABS2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row<N, ROW_INV_ABS2><<<grid, block, sm, st>>>(a);
+        break;
+    case ROW_INV_STORE:
+        cudaFuncSetAttribute(k_row<N, ROW_INV_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row<N, ROW_INV_STORE><<<grid, block, sm, st>>>(a);
+        break;
+    }
+}
+
+template <int N>
+static void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st)
+{
+    using L = FftLayout<N>;
+    dim3 grid((unsigned)(nwaves * (nx / L::TC))), block(L::COL_THREADS);
+    size_t sm = L::COL_SMEM;
+    switch (op) {
+    case COL_PROBE_INV:
+        cudaFuncSetAttribute(k_col<N, COL_PROBE_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_PROBE_INV><<<grid, block, sm, st>>>(a);
+        break;
+    case COL_STEP:
+        cudaFuncSetAttribute(k_col<N, COL_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_STEP><<<grid, block, sm, st>>>(a);
+        break;
+    case COL_INV:
+        cudaFuncSetAttribute(k_col<N, COL_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_INV><<<grid, block, sm, st>>>(a);
+        break;
+    case COL_CTF_INV:
+        cudaFuncSetAttribute(k_col<N, COL_CTF_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_CTF_INV><<<grid, block, sm, st>>>(a);
+        break;
+    }
+}
+
+void launch_row(int N, int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st)
+{
+    if (nwaves <= 0) return;
+    switch (N) {
+    case 128: row_dispatch<128>(op, a, nwaves, ny, st); break;
+    case 256: row_dispatch<256>(op, a, nwaves, ny, st); break;
+    case 512: row_dispatch<512>(op, a, nwaves, ny, st); break;
+    case 1024: row_dispatch<1024>(op, a, nwaves, ny, st); break;
+    case 2048: row_dispatch<2048>(op, a, nwaves, ny, st); break;
+    default: throw MsError(MS_ERR_UNSUPPORTED, "unsupported row length");
+    }
+    count_launch();
+    check_launch("row pass");
+}
+
+void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st)
+{
+    if (nwaves <= 0) return;
+    switch (N) {
+    case 128: col_dispatch<128>(op, a, nwaves, nx, st); break;
+    case 256: col_dispatch<256>(op, a, nwaves, nx, st); break;
+    case 512: col_dispatch<512>(op, a, nwaves, nx, st); break;
+    case 1024: col_dispatch<1024>(op, a, nwaves, nx, st); break;
+    case 2048: col_dispatch<2048>(op, a, nwaves, nx, st); break;
+    default: throw MsError(MS_ERR_UNSUPPORTED, "unsupported column length");
+    }
+    count_launch();
+    check_launch("column pass");
+}
+
+size_t row_smem(int N)
+{
+    switch (N) {
+    case 128: return FftLayout<128>::ROW_SMEM;
+    case 256: return FftLayout<256>::ROW_SMEM;
+    case 512: return FftLayout<512>::ROW_SMEM;
+    case 1024: return FftLayout<1024>::ROW_SMEM;
+    case 2048: return FftLayout<2048>::ROW_SMEM;
+    }
+    return 0;
+}
+size_t col_smem(int N)
+{
+    switch (N) {
+    case 128: return FftLayout<128>::COL_SMEM;
+    case 256: return FftLayout<256>::COL_SMEM;
+    case 512: return FftLayout<512>::COL_SMEM;
+    case 1024: return FftLayout<1024>::COL_SMEM;
+    case 2048: return FftLayout<2048>::COL_SMEM;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// projected potential: gen_slice_potential_kernel (device_kernels.cuh:28-47)
+// restructured as atom-culled 64x16 pixel tiles with float4 stores
+// ---------------------------------------------------------------------------
+constexpr int kPotTX = 64, kPotTY = 16, kPotThreads = 256, kPotMaxImg = 4;
+
+__device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
+{
+    // index of unrolledBinarySearch_c_nR (basic_functions_dev.cuh:47-67): the largest node
+    // i <= nR-2 with R2[i] <= r2 (or 0), from a log2 guess corrected by one comparison
+    float lr = __log2f(fmaxf(r2, 1e-30f));
+    int i = __float2int_rd((lr - T.l0) * T.inv_dl);
+    i = min(max(i, 0), MS_NR - 2);
+    if (r2 < T.R2[i]) i = max(i - 1, 0);
+    else if (i < MS_NR - 2 && r2 >= T.R2[i + 1]) i = i + 1;
+    float d = r2 - T.R2[i];
+    return ((T.c3[i] * d + T.c2[i]) * d + T.c1[i]) * d + T.c0[i];  // get_value_Cubic_Spline
+}
+
+__global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
+{
+    extern __shared__ __align__(16) unsigned char psm[];
+    ElemTable* el = reinterpret_cast<ElemTable*>(psm);
+    float4* cand = reinterpret_cast<float4*>(psm + sizeof(ElemTable) * a.n_elem);
+    __shared__ int wsum[kPotThreads / 32];
+    __shared__ int total_s;
+
+    const int conf = blockIdx.z;
+    const int sl = a.slice0 + blockIdx.y;
+    const int tiles_x = a.nx / kPotTX;
+    const int tx0 = (blockIdx.x % tiles_x) * kPotTX, ty0 = (blockIdx.x / tiles_x) * kPotTY;
+    const int t = threadIdx.x, px = t % (kPotTX / 4), py = t / (kPotTX / 4);
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+
+    if (sl < a.ns[conf]) {
+        {
+            const float4* src = reinterpret_cast<const float4*>(a.elems);
+            float4* dst = reinterpret_cast<float4*>(el);
+            int nv4 = (int)(sizeof(ElemTable) * a.n_elem / 16);
+            for (int i = t; i < nv4; i += kPotThreads) dst[i] = src[i];
+        }
+        __syncthreads();
+        const int64_t s0 = a.seg[(int64_t)conf * (a.S_cap + 1) + sl];
+        const int64_t s1 = a.seg[(int64_t)conf * (a.S_cap + 1) + sl + 1];
+        const float X0 = (float)tx0 * a.dx, X1 = (float)(tx0 + kPotTX - 1) * a.dx;
+        const float Y0 = (float)ty0 * a.dy, Y1 = (float)(ty0 + kPotTY - 1) * a.dy;
+        const float Y = (float)(ty0 + py) * a.dy;
+        float X[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) X[k] = (float)(tx0 + 4 * px + k) * a.dx;
+        const int lane = t & 31, wid = t >> 5;
+        for (int64_t base = s0; base < s1; base += kPotThreads) {
+            int64_t i = base + t;
+            float4 cimg[kPotMaxImg];
+            int cnt = 0;
+            if (i < s1) {
+                float xa = a.ax[i], ya = a.ay[i], w = a.aw[i];
+                int e = a.ae[i];
+                float rm = el[e].rmax * 1.0001f + 1e-4f;
+                const int lo = a.wrap ? -1 : 0, hi = a.wrap ? 1 : 0;
+                for (int iy = lo; iy <= hi; iy++)
+                    for (int ix = lo; ix <= hi; ix++) {
+                        float xs = xa + ix * a.lx, ys = ya + iy * a.ly;
+                        float dxr = fmaxf(0.f, fmaxf(X0 - xs, xs - X1));
+                        float dyr = fmaxf(0.f, fmaxf(Y0 - ys, ys - Y1));
+                        if (dxr * dxr + dyr * dyr < rm * rm && cnt < kPotMaxImg)
+                            cimg[cnt++] = make_float4(xs, ys, w, __int_as_float(e));
+                    }
+            }
+            // ordered compaction (deterministic: atom order, then image order)
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) wsum[wid] = incl;
+            __syncthreads();
+            if (t == 0) {
+                int run = 0;
+                for (int w = 0; w < kPotThreads / 32; w++) {
+                    int v = wsum[w];
+                    wsum[w] = run;
+                    run += v;
+                }
+                total_s = run;
+            }
+            __syncthreads();
+            int off = wsum[wid] + incl - cnt;
+            for (int q = 0; q < cnt; q++) cand[off + q] = cimg[q];
+            __syncthreads();
+            const int total = total_s;
+            for (int q = 0; q < total; q++) {
+                float4 cd = cand[q];
+                const ElemTable& T = el[__float_as_int(cd.w)];
+                float dy = Y - cd.y;
+                float dy2 = dy * dy;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    float dx = X[k] - cd.x;
+                    float r2 = dx * dx + dy2;
+                    if (r2 < T.rmax2) acc[k] += cd.z * spline_eval(T, r2);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (sl < a.slice0 + a.nslice) {
+        float* out = a.V + (int64_t)conf * a.V_conf_stride + (int64_t)(sl - a.V_slice_base) * a.nx * a.ny +
+                     (int64_t)(ty0 + py) * a.nx + tx0 + 4 * px;
+        *reinterpret_cast<float4*>(out) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    }
+}
+
+void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st)
+{
+    if (a.nslice <= 0 || n_conf <= 0) return;
+    dim3 grid((unsigned)((a.nx / kPotTX) * (a.ny / kPotTY)), (unsigned)a.nslice, (unsigned)n_conf);
+    size_t sm = sizeof(ElemTable) * a.n_elem + sizeof(float4) * kPotThreads * kPotMaxImg;
+    cudaFuncSetAttribute(k_potential, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_potential<<<grid, kPotThreads, sm, st>>>(a);
+    count_launch();
+    check_launch("potential");
+}
+
+// ---------------------------------------------------------------------------
+// specimen on the device: displacement, z range, slice assignment, gather
+// ---------------------------------------------------------------------------
+__global__ void k_displace(const float* x, const float* y, const float* z, const float* sig, int64_t n,
+                           const int* confs, uint64_t seed, int dx, int dy, int dzf, float* xd, float* yd, float* zd)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int ci = blockIdx.y;
+    float xi = x[i], yi = y[i], zi = z[i];
+    det_displace(seed, confs[ci], i, sig[i], dx, dy, dzf, &xi, &yi, &zi);
+    int64_t o = (int64_t)ci * n + i;
+    xd[o] = xi;
+    yd[o] = yi;
+    zd[o] = zi;
+}
+
+void launch_displace(const float* x, const float* y, const float* z, const float* sig, int64_t n, const int* confs,
+                     int nconf, uint64_t seed, int dx, int dy, int dzf, float* xd, float* yd, float* zd,
+                     cudaStream_t st)
+{
+    dim3 grid((unsigned)((n + 255) / 256), (unsigned)nconf);
+    k_displace<<<grid, 256, 0, st>>>(x, y, z, sig, n, confs, seed, dx, dy, dzf, xd, yd, zd);
+    count_launch();
+    check_launch("displace");
+}
+
+__device__ __forceinline__ unsigned f2ord(float f)
+{
+    unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__global__ void k_zrange(const float* zd, int64_t n, unsigned* zmin, unsigned* zmax)
+{
+    int ci = blockIdx.y;
+    unsigned lo = 0xFFFFFFFFu, hi = 0u;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        unsigned k = f2ord(zd[(int64_t)ci * n + i]);
+        lo = min(lo, k);
+        hi = max(hi, k);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(zmin + ci, lo);
+        atomicMax(zmax + ci, hi);
+    }
+}
+
+void launch_zrange(const float* zd, int64_t n, int nconf, unsigned* zmin_bits, unsigned* zmax_bits, cudaStream_t st)
+{
+    cudaMemsetAsync(zmin_bits, 0xFF, sizeof(unsigned) * nconf, st);
+    cudaMemsetAsync(zmax_bits, 0x00, sizeof(unsigned) * nconf, st);
+    int blocks = (int)std::min<int64_t>(1184, (n + 255) / 256);
+    k_zrange<<<dim3(blocks, nconf), 256, 0, st>>>(zd, n, zmin_bits, zmax_bits);
+    count_launch();
+    check_launch("z range");
+}
+
+__global__ void k_assign(const float* zd, int64_t n, const float* bounds, int bstride, const int* nv,
+                         const float* vmax, int S_cap, unsigned* keys, int* vals, unsigned* counts)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int ci = blockIdx.y;
+    int s = det_slice_of(zd[(int64_t)ci * n + i], bounds + (int64_t)ci * bstride, nv[ci], vmax[ci]);
+    unsigned key = (unsigned)ci * (unsigned)(S_cap + 1) + (unsigned)(s >= 0 ? s : S_cap);
+    keys[(int64_t)ci * n + i] = key;
+    vals[(int64_t)ci * n + i] = (int)i;
+    atomicAdd(counts + key, 1u);
+}
+
+void launch_assign(const float* zd, int64_t n, int nconf, const float* bounds, int bstride, const int* nv,
+                   const float* vmax, int S_cap, unsigned* keys, int* vals, unsigned* counts, cudaStream_t st)
+{
+    dim3 grid((unsigned)((n + 255) / 256), (unsigned)nconf);
+    k_assign<<<grid, 256, 0, st>>>(zd, n, bounds, bstride, nv, vmax, S_cap, keys, vals, counts);
+    count_launch();
+    check_launch("slice assignment");
+}
+
+__global__ void k_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const float* xd,
+                         const float* yd, const float* occ, const int* elem, float vr, float* ax, float* ay, float* aw,
+                         int* ae)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    unsigned key = keys[i];
+    int64_t ci = key / (unsigned)(S_cap + 1);
+    int64_t at = vals[i];
+    ax[i] = xd[ci * n + at];
+    ay[i] = yd[ci * n + at];
+    aw[i] = vr * occ[at];
+    ae[i] = elem[at];
+}
+
+void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const float* xd,
+                   const float* yd, const float* occ, const int* elem, float vr_factor, float* ax, float* ay,
+                   float* aw, int* ae, cudaStream_t st)
+{
+    k_gather<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(keys, vals, total, n, S_cap, xd, yd, occ, elem,
+                                                              vr_factor, ax, ay, aw, ae);
+    count_launch();
+    check_launch("gather");
+}
+
+// ---------------------------------------------------------------------------
+// post-processing
+// ---------------------------------------------------------------------------
+constexpr int kDetThreads = 256;
+
+// sum_square_over_Det_batch (device_kernels.cuh:625-671): annular sums of |Psi|^2 per wave,
+// accumulated in FP64 per thread and reduced in a fixed order.
+__global__ void __launch_bounds__(kDetThreads) k_detect(const float2* psi, int nx, int ny, float dgx, float dgy,
+                                                        const float* g2in, const float* g2out, int ndet,
+                                                        double* partial)
+{
+    __shared__ double red[MS_MAX_DET][kDetThreads / 32];
+    const int b = blockIdx.y;
+    const int64_t N = (int64_t)nx * ny;
+    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
+    const int64_t p0 = per * blockIdx.x, p1 = min(N, p0 + per);
+    float gi[MS_MAX_DET], go[MS_MAX_DET];
+    double acc[MS_MAX_DET];
+#pragma unroll
+    for (int d = 0; d < MS_MAX_DET; d++) {
+        gi[d] = d < ndet ? g2in[d] : 1.f;
+        go[d] = d < ndet ? g2out[d] : 0.f;
+        acc[d] = 0.0;
+    }
+    const float2* w = psi + (int64_t)b * N;
+    for (int64_t p = p0 + threadIdx.x; p < p1; p += kDetThreads) {
+        int ix = (int)(p % nx), iy = (int)(p / nx);
+        float g2 = det_g2(ix, iy, nx, ny, dgx, dgy);
+        float2 v = w[p];
+        double a2 = (double)v.x * v.x + (double)v.y * v.y;
+#pragma unroll
+        for (int d = 0; d < MS_MAX_DET; d++)
+            if (gi[d] <= g2 && g2 <= go[d]) acc[d] += a2;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < MS_MAX_DET; d++) {
+        double v = acc[d];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[d][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < ndet) {
+        double s = 0.0;
+        for (int k = 0; k < kDetThreads / 32; k++) s += red[threadIdx.x][k];
+        partial[((int64_t)b * gridDim.x + blockIdx.x) * ndet + threadIdx.x] = s;
+    }
+}
+
+void launch_detect(const float2* psi, int nwaves, int nx, int ny, float dgx, float dgy, const float* g2in,
+                   const float* g2out, int ndet, double* partial, int nblk, cudaStream_t st)
+{
+    k_detect<<<dim3(nblk, nwaves), kDetThreads, 0, st>>>(psi, nx, ny, dgx, dgy, g2in, g2out, ndet, partial);
+    count_launch();
+    check_launch("detector");
+}
+
+__global__ void k_det_finalize(const double* partial, int nwaves, int nblk, int ndet, const WaveInfo* waves,
+                               double* I_wave, double* image, int npos, int accumulate)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nwaves * ndet) return;
+    int b = i / ndet, d = i % ndet;
+    double s = 0.0;
+    for (int k = 0; k < nblk; k++) s += partial[((int64_t)b * nblk + k) * ndet + d];
+    if (I_wave) I_wave[i] = s;
+    if (image) {
+        double v = (double)waves[b].weight * s;
+        int64_t o = (int64_t)d * npos + waves[b].pos;
+        image[o] = accumulate ? image[o] + v : v;
+    }
+}
+
+void launch_det_finalize(const double* partial, int nwaves, int nblk, int ndet, const WaveInfo* waves,
+                         double* I_wave, double* image, int npos, int accumulate, cudaStream_t st)
+{
+    int n = nwaves * ndet;
+    k_det_finalize<<<(n + 127) / 128, 128, 0, st>>>(partial, nwaves, nblk, ndet, waves, I_wave, image, npos,
+                                                     accumulate);
+    count_launch();
+    check_launch("detector finalize");
+}
+
+// add_scale_square / add_scale_components / add_weighted_scale over configurations
+// (device_kernels.cuh:296-329), accumulated in FP64 in wave order.
+__global__ void k_acc_abs2(const float2* psi, int nwaves, const WaveInfo* waves, int64_t N, double* acc, int first)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    double s = first ? 0.0 : acc[p];
+    for (int b = 0; b < nwaves; b++) {
+        float2 v = psi[(int64_t)b * N + p];
+        s += (double)waves[b].weight * ((double)v.x * v.x + (double)v.y * v.y);
+    }
+    acc[p] = s;
+}
+
+void launch_acc_abs2(const float2* psi, int nwaves, const WaveInfo* waves, int64_t N, double* acc, int first,
+                     cudaStream_t st)
+{
+    k_acc_abs2<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(psi, nwaves, waves, N, acc, first);
+    count_launch();
+    check_launch("accumulate |psi|^2");
+}
+
+__global__ void k_acc_cplx(const float2* psi, int nwaves, const WaveInfo* waves, int64_t N, double* re, double* im,
+                           int first)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    double sr = first ? 0.0 : re[p], si = first ? 0.0 : im[p];
+    for (int b = 0; b < nwaves; b++) {
+        float2 v = psi[(int64_t)b * N + p];
+        sr += (double)waves[b].weight * v.x;
+        si += (double)waves[b].weight * v.y;
+    }
+    re[p] = sr;
+    im[p] = si;
+}
+
+void launch_acc_cplx(const float2* psi, int nwaves, const WaveInfo* waves, int64_t N, double* re, double* im,
+                     int first, cudaStream_t st)
+{
+    k_acc_cplx<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(psi, nwaves, waves, N, re, im, first);
+    count_launch();
+    check_launch("accumulate wave");
+}
+
+__global__ void k_acc_real(const float* in, int nwaves, int64_t N, double* acc, int first)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    double s = first ? 0.0 : acc[p];
+    for (int b = 0; b < nwaves; b++) s += (double)in[(int64_t)b * N + p];
+    acc[p] = s;
+}
+
+void launch_acc_real(const float* in, int nwaves, int64_t N, double* acc, int first, cudaStream_t st)
+{
+    k_acc_real<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(in, nwaves, N, acc, first);
+    count_launch();
+    check_launch("accumulate image");
+}
+
+// FP64 accumulator -> float output, optionally quadrant-swapped (fft_shift, device_kernels.cuh:342-362)
+__global__ void k_emit(const double* acc, int nx, int ny, int shift, float* out)
+{
+    int64_t N = (int64_t)nx * ny;
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    int ix = (int)(p % nx), iy = (int)(p / nx);
+    int64_t q = shift ? (int64_t)((iy + ny / 2) % ny) * nx + (ix + nx / 2) % nx : p;
+    out[q] = (float)acc[p];
+}
+
+void launch_emit(const double* acc, int nx, int ny, int shift, float* out, cudaStream_t st)
+{
+    int64_t N = (int64_t)nx * ny;
+    k_emit<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(acc, nx, ny, shift, out);
+    count_launch();
+    check_launch("emit");
+}
+
+__global__ void k_d2f(const double* in, int64_t n, float* out)
+{
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) out[p] = (float)in[p];
+}
+
+void launch_d2f(const double* in, int64_t n, float* out, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_d2f<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, n, out);
+    count_launch();
+    check_launch("convert");
+}
+
+// seg[0] = 0, seg[i+1] = seg[i] + counts[i]: one block, chunked sequential sums
+__global__ void k_scan_counts(const unsigned* counts, int n, int64_t* seg)
+{
+    __shared__ int64_t part[1024];
+    const int t = threadIdx.x, T = blockDim.x;
+    const int per = (n + T - 1) / T;
+    const int i0 = min(n, t * per), i1 = min(n, i0 + per);
+    int64_t s = 0;
+    for (int i = i0; i < i1; i++) s += counts[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        int64_t run = 0;
+        for (int k = 0; k < T; k++) {
+            int64_t v = part[k];
+            part[k] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    int64_t run = part[t];
+    if (t == 0) seg[0] = 0;
+    for (int i = i0; i < i1; i++) {
+        run += counts[i];
+        seg[i + 1] = run;
+    }
+}
+
+void launch_scan_counts(const unsigned* counts, int n, int64_t* seg, cudaStream_t st)
+{
+    k_scan_counts<<<1, 1024, 0, st>>>(counts, n, seg);
+    count_launch();
+    check_launch("scan");
+}
+
+__global__ void k_fill_c(float2* p, int64_t n, float2 v)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+void launch_fill_c(float2* p, int64_t n, float2 v, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_fill_c<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+    count_launch();
+    check_launch("fill");
+}
+
+}  // namespace msb

@@ -1,0 +1,121 @@
+// Device data structures and launchers of the engine's kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "engine.hpp"
+
+namespace msb {
+
+// One wave of a batch.
+struct WaveInfo {
+    double px, py;   // probe position, Angstrom
+    double cc10;     // -pi (C10 + z_init) lambda of the probe, gated like Lens_Dev
+    int conf_slot;   // which potential slot (configuration) the wave reads
+    int n_slices;    // slices of the wave's specimen
+    float weight;    // configuration weight
+    int pos;         // output index (scan position) of the wave
+};
+
+struct GridDev {
+    int nx, ny;
+    float dgx_f, dgy_f;
+    double dgx, dgy;
+    float gl2_f, alpha_f;
+    int bwl;
+    float inv_n;
+};
+
+struct LensDev {
+    int m, phi_req;
+    double cc10, cc12, cc21, cc23, cc30, cc32, cc34, cc41, cc43, cc45, cc50, cc52, cc54, cc56;
+    double p12, p21, p23, p32, p34, p41, p43, p45, p52, p54, p56;
+    float g2min, g2max;
+};
+
+enum RowOp { ROW_T_FWD = 0, ROW_INV_T_FWD = 1, ROW_INV_ABS2 = 2, ROW_INV_STORE = 3 };
+enum ColOp { COL_PROBE_INV = 0, COL_STEP = 1, COL_INV = 2, COL_CTF_INV = 3 };
+
+enum PassFlags {
+    PF_VACUUM_BEYOND = 1,  // slices past a wave's own count are empty (t = 1) instead of skipped
+    PF_ACCUMULATE = 2,     // ROW_INV_ABS2 adds into its output
+    PF_FILTER_AUX = 4,     // COL_STEP also writes the annulus-filtered spectrum to aux
+    PF_PROP_ALWAYS = 8     // COL_STEP propagates even after the wave's last slice
+};
+
+struct PassArgs {
+    float2* psi;            // [B][ny][nx]
+    float2* aux;            // [B][ny][nx] (filtered branch, complex outputs)
+    float* out_real;        // [B][ny][nx] or a frame
+    const WaveInfo* waves;  // [B]
+    int slice;
+    int flags;
+    const float* sV;          // potential store, [slot][slice][ny][nx], rad
+    int64_t sV_slot_stride;   // floats per slot
+    int sV_slice_base;        // slice index held at the store's slice 0
+    const float2* tw;         // inter-level twiddles for this pass's length
+    const float2* prop_x;     // [nx] exp(i w (gx - g0x)^2)
+    const float2* prop_y;     // [ny] exp(i w (gy - g0y)^2)
+    GridDev grid;
+    LensDev lens;
+    float filt_g2in, filt_g2out;
+};
+
+// Sorted atoms of a group of configurations.
+struct PotArgs {
+    const float* ax;
+    const float* ay;
+    const float* aw;            // Vr_factor * occupancy
+    const int* ae;              // element index
+    const int64_t* seg;         // [n_conf][S_cap + 1] start offsets, seg[.][S_cap] = end
+    const int* ns;              // slices per configuration
+    int S_cap;                  // slice slots per configuration
+    int slice0, nslice;         // slices computed by this launch
+    float* V;                   // [n_conf][S_cap][ny][nx] (or [n_conf][nslice][...] with slice0 offset)
+    int64_t V_conf_stride;      // floats per configuration in V
+    int V_slice_base;           // slice index stored at V's slice 0
+    int nx, ny;
+    float dx, dy, lx, ly;
+    int wrap;
+    const ElemTable* elems;
+    int n_elem;
+};
+
+// launchers (kernels.cu); all asynchronous on `st`
+void upload_constants(cudaStream_t st);
+void launch_row(int N, int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st);
+void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
+size_t row_smem(int N);
+size_t col_smem(int N);
+void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st);
+
+// specimen on the device
+void launch_displace(const float* x, const float* y, const float* z, const float* sig, int64_t n, const int* confs,
+                     int nconf, uint64_t seed, int dx, int dy, int dzf, float* xd, float* yd, float* zd,
+                     cudaStream_t st);
+void launch_zrange(const float* zd, int64_t n, int nconf, unsigned* zmin_bits, unsigned* zmax_bits, cudaStream_t st);
+void launch_assign(const float* zd, int64_t n, int nconf, const float* bounds, int bstride, const int* nv,
+                   const float* vmax, int S_cap, unsigned* keys, int* vals, unsigned* counts, cudaStream_t st);
+void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const float* xd,
+                   const float* yd, const float* occ, const int* elem, float vr_factor, float* ax, float* ay,
+                   float* aw, int* ae, cudaStream_t st);
+
+// post-processing
+void launch_detect(const float2* psi, int nwaves, int nx, int ny, float dgx, float dgy, const float* g2in,
+                   const float* g2out, int ndet, double* partial, int nblk, cudaStream_t st);
+void launch_det_finalize(const double* partial, int nwaves, int nblk, int ndet, const WaveInfo* waves,
+                         double* I_wave, double* image, int npos, int accumulate, cudaStream_t st);
+void launch_acc_abs2(const float2* psi, int nwaves, const WaveInfo* waves, int64_t N, double* acc, int first,
+                     cudaStream_t st);
+void launch_acc_cplx(const float2* psi, int nwaves, const WaveInfo* waves, int64_t N, double* re, double* im,
+                     int first, cudaStream_t st);
+void launch_acc_real(const float* in, int nwaves, int64_t N, double* acc, int first, cudaStream_t st);
+void launch_emit(const double* acc, int nx, int ny, int shift, float* out, cudaStream_t st);
+void launch_d2f(const double* in, int64_t n, float* out, cudaStream_t st);
+void launch_scan_counts(const unsigned* counts, int n, int64_t* seg, cudaStream_t st);
+void launch_fill_c(float2* p, int64_t n, float2 v, cudaStream_t st);
+
+int64_t kernel_launches();     // running count of this library's launches
+void reset_kernel_launches();
+
+}  // namespace msb

@@ -1,0 +1,1184 @@
+/*
+ * ms_oracle.c -- TEST INFRASTRUCTURE ONLY (see ms_oracle.h).
+ *
+ * An FP64 restatement of cudaEM's multislice operators, written from the
+ * reference's source.  Each function cites the reference lines it follows.
+ * The arithmetic that must agree bit-for-bit with the CUDA engine (the
+ * phonon random numbers, the slicing planes, the aperture and detector
+ * masks) is done here in the same IEEE operations the engine uses, with
+ * floating-point contraction disabled at compile time.  Everything else is
+ * computed in double precision.
+ *
+ * Compile with -ffp-contract=off (oracle/Makefile does).
+ */
+#include "ms_oracle.h"
+
+#include <complex.h>
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define OR_PI 3.14159265358979323846264338327950288
+typedef double complex cplx;
+
+static int g_threads = 0;
+void or_set_threads(int n) { g_threads = n; }
+int or_get_threads(void)
+{
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* physics: relativistic wavelength, interaction constant.  The reference's   */
+/* get_Vr_factor lives in a missing header (transmission_function.cuh:60-61); */
+/* these are the textbook expressions with CODATA 2018 constants.             */
+/* ------------------------------------------------------------------------ */
+static const double C_H = 6.62607015e-34;     /* J s */
+static const double C_ME = 9.1093837015e-31;  /* kg */
+static const double C_QE = 1.602176634e-19;   /* C */
+static const double C_C = 299792458.0;        /* m/s */
+
+void or_physics(double E0_kV, double* lambda, double* sigma, double* gamma)
+{
+    double E = E0_kV * 1e3;
+    double g = 1.0 + C_QE * E / (C_ME * C_C * C_C);
+    double lam = C_H / sqrt(2.0 * C_ME * C_QE * E * (1.0 + C_QE * E / (2.0 * C_ME * C_C * C_C)));
+    if (lambda) *lambda = lam * 1e10;
+    if (sigma) *sigma = 2.0 * OR_PI * g * C_ME * C_QE * lam / (C_H * C_H) * 1e-10;
+    if (gamma) *gamma = g;
+}
+
+/* ------------------------------------------------------------------------ */
+/* frozen-phonon random numbers.  The reference's vibrate_atom_positions and  */
+/* random_lib.hpp are missing (single_simulator.cuh:65-74); this is the       */
+/* engine's own counter-based generator: SplitMix64 mixing of                 */
+/* (seed, conf, atom, stream), Marsaglia's polar method, and a logarithm      */
+/* built only from IEEE-exact operations so that host and device agree bit    */
+/* for bit.                                                                   */
+/* ------------------------------------------------------------------------ */
+static uint64_t or_mix(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+double or_det_log(double s)
+{
+    /* s = m 2^e with m in [sqrt(1/2), sqrt(2)); log m = 2 atanh(t), t = (m-1)/(m+1),
+       summed as the Maclaurin series of atanh to t^27 (|t| <= 0.1716). */
+    int e;
+    double m = frexp(s, &e);
+    if (m < 0.70710678118654752440) {
+        m = m * 2.0;
+        e = e - 1;
+    }
+    double t = (m - 1.0) / (m + 1.0);
+    double t2 = t * t;
+    double q = 1.0 / 27.0;
+    q = q * t2 + 1.0 / 25.0;
+    q = q * t2 + 1.0 / 23.0;
+    q = q * t2 + 1.0 / 21.0;
+    q = q * t2 + 1.0 / 19.0;
+    q = q * t2 + 1.0 / 17.0;
+    q = q * t2 + 1.0 / 15.0;
+    q = q * t2 + 1.0 / 13.0;
+    q = q * t2 + 1.0 / 11.0;
+    q = q * t2 + 1.0 / 9.0;
+    q = q * t2 + 1.0 / 7.0;
+    q = q * t2 + 1.0 / 5.0;
+    q = q * t2 + 1.0 / 3.0;
+    q = q * t2 + 1.0;
+    double lm = 2.0 * t * q;
+    return (double)e * 0.69314718055994530942 + lm;
+}
+
+void or_gauss_pair(uint64_t seed, int conf, int64_t atom, int stream, double* g0, double* g1)
+{
+    uint64_t key = or_mix(or_mix(or_mix(seed) ^ (uint64_t)(int64_t)conf) ^
+                          (((uint64_t)atom << 2) | (uint64_t)stream));
+    for (int it = 0; it < 64; it++) {
+        uint64_t r0 = or_mix(key + (uint64_t)(2 * it));
+        uint64_t r1 = or_mix(key + (uint64_t)(2 * it + 1));
+        double u = ((double)(r0 >> 11) + 0.5) * 0x1.0p-53;
+        double v = ((double)(r1 >> 11) + 0.5) * 0x1.0p-53;
+        u = 2.0 * u - 1.0;
+        v = 2.0 * v - 1.0;
+        double s = u * u + v * v;
+        if (s < 1.0 && s > 0.0) {
+            double f = sqrt(-2.0 * or_det_log(s) / s);
+            *g0 = u * f;
+            *g1 = v * f;
+            return;
+        }
+    }
+    *g0 = 0.0;
+    *g1 = 0.0;
+}
+
+/* Displacement of configuration conf >= 1; conf 0 is the static specimen. */
+void or_displace(const ms_params* p, const ms_atoms* a, int conf, float* x, float* y, float* z)
+{
+    for (int64_t i = 0; i < a->n; i++) {
+        float xi = a->x[i], yi = a->y[i], zi = a->z[i];
+        if (conf > 0) {
+            double g0, g1, g2, g3;
+            or_gauss_pair(p->pn_seed, conf, i, 0, &g0, &g1);
+            or_gauss_pair(p->pn_seed, conf, i, 1, &g2, &g3);
+            double s = (double)a->sigma[i];
+            if (p->pn_dim_x) xi = xi + (float)(s * g0);
+            if (p->pn_dim_y) yi = yi + (float)(s * g1);
+            if (p->pn_dim_z) zi = zi + (float)(s * g2);
+        }
+        x[i] = xi;
+        y[i] = yi;
+        z[i] = zi;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* slicing: Slice_Generator::gene_bounds / get_slicing / fd_by_z             */
+/* (slice_generator.hpp:56-168), in float like the reference's T = float.     */
+/* z_eps is epsilon_rel<float>() of the missing host header, taken as 1e-4    */
+/* (the relative epsilon of the reference's float compare, misc_dev.cuh:17-23)*/
+/* ------------------------------------------------------------------------ */
+static int or_border(const ms_params* p)
+{
+    if (p->slice_border >= 0) return p->slice_border;
+    return p->simulation_type == MS_SIM_HRTEM ? MS_BORDER_MAX : MS_BORDER_MIN; /* specimen.cuh:24-35 */
+}
+
+int or_slices(const ms_params* p, const float* z, int64_t n, float* bounds, int cap, int* atom_slice)
+{
+    const float z_eps = 1e-4f;
+    const float dz = (float)p->dz;
+    if (n <= 0) return 0;
+    float vmin = z[0], vmax = z[0];
+    for (int64_t i = 1; i < n; i++) {
+        if (z[i] < vmin) vmin = z[i];
+        if (z[i] > vmax) vmax = z[i];
+    }
+    float s_v = vmax - vmin;
+    int nv = (int)floorf((s_v + z_eps) / dz) + 2;
+    float* b = (float*)malloc(sizeof(float) * (size_t)nv);
+    int border = or_border(p);
+    if (border == MS_BORDER_MIN) {
+        float zb = vmin - 2 * z_eps;
+        for (int i = 0; i < nv; i++) b[i] = zb + (float)i * dz;
+    } else if (border == MS_BORDER_MAX) {
+        float zt = vmax + 2 * z_eps;
+        for (int i = 0; i < nv; i++) b[nv - 1 - i] = zt - (float)i * dz;
+    } else {
+        float zb = 0.5f * (vmin + vmax - (float)(nv - 1) * dz);
+        for (int i = 0; i < nv; i++) b[i] = zb + (float)i * dz;
+    }
+    int ns = nv - 1;
+    if (bounds)
+        for (int i = 0; i < nv && i < cap; i++) bounds[i] = b[i];
+    if (atom_slice) {
+        /* slice i holds bound[i] <= z < bound[i+1]; the top atom equal to the last plane
+           belongs to the last slice (fd_by_z, slice_generator.hpp:109-129). */
+        for (int64_t k = 0; k < n; k++) {
+            float zk = z[k];
+            int s = -1;
+            if (zk >= b[0] && zk < b[nv - 1]) {
+                int lo = 0, hi = nv - 1; /* largest i with b[i] <= zk */
+                while (hi - lo > 1) {
+                    int mid = (lo + hi) / 2;
+                    if (b[mid] <= zk) lo = mid; else hi = mid;
+                }
+                s = lo;
+            } else if (zk == b[nv - 1] && zk == vmax) {
+                s = ns - 1;
+            }
+            atom_slice[k] = s;
+        }
+    }
+    free(b);
+    return ns;
+}
+
+/* ------------------------------------------------------------------------ */
+/* element potentials.  V(r) and V'(r) in the reference's functional forms   */
+/* (basic_functions_dev.cuh:102-186); the default table is Moliere's          */
+/* Thomas-Fermi screening approximation written in the Kirkland form (three   */
+/* Yukawa terms): V(r) = (e^2/4 pi eps0) Z/r sum a_i exp(-b_i r/a_TF),         */
+/* a_i = (0.35, 0.55, 0.10), b_i = (0.3, 1.2, 6.0), a_TF = 0.88534 a0 Z^-1/3.   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int form;
+    int n;
+    double cl[MS_MAX_COEF], cnl[MS_MAX_COEF];
+} or_coef;
+
+static void or_moliere(int Z, or_coef* c)
+{
+    const double a0 = 0.529177210903;                    /* Bohr radius, A */
+    const double ke = 14.399645478425668;                /* e^2/(4 pi eps0), eV A */
+    const double tf = 0.88534138;                        /* (9 pi^2 / 128)^(1/3) */
+    double aTF = tf * a0 * pow((double)Z, -1.0 / 3.0);
+    const double al[3] = {0.35, 0.55, 0.10}, be[3] = {0.3, 1.2, 6.0};
+    memset(c, 0, sizeof(*c));
+    c->form = MS_POT_KIRKLAND_0_12;
+    c->n = 6;
+    for (int i = 0; i < 3; i++) {
+        c->cl[i] = ke * Z * al[i];
+        c->cnl[i] = be[i] / aTF;
+    }
+    for (int i = 3; i < 6; i++) {
+        c->cl[i] = 0.0;
+        c->cnl[i] = 1.0;
+    }
+}
+
+static void or_coef_for(const ms_params* p, int Z, or_coef* c)
+{
+    for (int i = 0; i < p->n_element_coefs; i++) {
+        const ms_element_coef* e = &p->element_coefs[i];
+        if (e->Z == Z) {
+            memset(c, 0, sizeof(*c));
+            c->form = e->form;
+            c->n = (e->form == MS_POT_DOYLE_0_4) ? 4 : (e->form == MS_POT_PENG_0_4 || e->form == MS_POT_PENG_0_12 ||
+                                                      e->form == MS_POT_LOBATO_0_12) ? 5 : 6;
+            for (int k = 0; k < MS_MAX_COEF; k++) {
+                c->cl[k] = e->cl[k];
+                c->cnl[k] = e->cnl[k];
+            }
+            return;
+        }
+    }
+    or_moliere(Z, c);
+}
+
+/* V(r) and V'(r) (note: the reference returns dVrir = V'(r)/r) */
+static void or_Vr(const or_coef* c, double r, double* V, double* dV)
+{
+    double v = 0.0, d = 0.0;
+    switch (c->form) {
+    case MS_POT_DOYLE_0_4:
+    case MS_POT_PENG_0_4:
+    case MS_POT_PENG_0_12: {
+        int n = (c->form == MS_POT_DOYLE_0_4) ? 4 : 5;
+        for (int i = 0; i < n; i++) {
+            double e = c->cl[i] * exp(-c->cnl[i] * r * r);
+            v += e;
+            d += -2.0 * c->cnl[i] * r * e;
+        }
+    } break;
+    case MS_POT_KIRKLAND_0_12:
+    case MS_POT_MOLIERE: {
+        for (int i = 0; i < 3; i++) {
+            double e = c->cl[i] * exp(-c->cnl[i] * r) / r;
+            v += e;
+            d += -e * (c->cnl[i] + 1.0 / r);
+        }
+        for (int i = 3; i < 6; i++) {
+            double e = c->cl[i] * exp(-c->cnl[i] * r * r);
+            v += e;
+            d += -2.0 * c->cnl[i] * r * e;
+        }
+    } break;
+    case MS_POT_WEICKENMEIER_0_12: {
+        double s = 0.0, sd = 0.0;
+        for (int i = 0; i < 6; i++) {
+            s += c->cl[i] * erfc(c->cnl[i] * r);
+            sd += c->cl[i] * c->cnl[i] * exp(-c->cnl[i] * c->cnl[i] * r * r);
+        }
+        v = s / r;
+        d = -(2.0 * sd / 1.772453850905516027298) / r - s / (r * r);
+    } break;
+    case MS_POT_LOBATO_0_12: {
+        for (int i = 0; i < 5; i++) {
+            double br = c->cnl[i] * r;
+            double e = c->cl[i] * exp(-br);
+            v += e * (2.0 / br + 1.0);
+            d += -e * (2.0 / (br * r) + 2.0 / r + c->cnl[i]);
+        }
+    } break;
+    default:
+        break;
+    }
+    *V = v;
+    *dV = d;
+}
+
+/* V_z(R) = 2 int_0^inf V(R cosh u) R cosh u du ; dV_z/dR^2 = int_0^inf V'(R cosh u) du.
+   Trapezoid rule in u (exponentially convergent for these integrands). */
+static void or_project(const or_coef* c, double R, double* Vz, double* dVz)
+{
+    const double h = 0.02;
+    double sv = 0.0, sd = 0.0;
+    double V, dV;
+    or_Vr(c, R, &V, &dV);
+    sv = 0.5 * V * R;
+    sd = 0.5 * dV;
+    for (int k = 1; k < 4000; k++) {
+        double ch = cosh(k * h);
+        double r = R * ch;
+        or_Vr(c, r, &V, &dV);
+        double tv = V * r, td = dV;
+        sv += tv;
+        sd += td;
+        if (fabs(tv) < 1e-18 * fabs(sv) && fabs(td) < 1e-18 * fabs(sd) && k > 10) break;
+    }
+    *Vz = 2.0 * h * sv;
+    *dVz = h * sd;
+}
+
+int or_projected(const ms_params* p, int Z, double R, double* Vz, double* dVz_dR2)
+{
+    or_coef c;
+    or_coef_for(p, Z, &c);
+    or_project(&c, R, Vz, dVz_dR2);
+    return 0;
+}
+
+static double or_rmin(const ms_params* p) { return p->pot_rmin > 0 ? p->pot_rmin : 0.01; }
+static double or_rmax(const ms_params* p) { return p->pot_rmax > 0 ? p->pot_rmax : 3.0; }
+
+/* Radial spline table (the VR_Cubic coefficients of Element_Coeffs,
+   device_containers.cuh:243-249): log-spaced nodes in R, values and
+   derivatives in R^2, a cosine taper in R^2 from R_tap = 0.85 R_max
+   (apply_tapering_dev, basic_functions_dev.cuh:90-101) and Hermite cubic
+   coefficients (get_cubic_poly_coef, basic_functions_dev.cuh:76-89). */
+int or_spline(const ms_params* p, int Z, double* R2, double* c0, double* c1, double* c2, double* c3, double* rmax)
+{
+    or_coef c;
+    or_coef_for(p, Z, &c);
+    double rmn = or_rmin(p), rmx = or_rmax(p);
+    double R2tap = (0.85 * rmx) * (0.85 * rmx);
+    double tap_cf = OR_PI / (2.0 * (rmx * rmx - R2tap));
+    for (int i = 0; i < MS_NR; i++) {
+        double R = rmn * pow(rmx / rmn, (double)i / (double)(MS_NR - 1));
+        if (i == MS_NR - 1) R = rmx;
+        double Vz, dVz;
+        or_project(&c, R, &Vz, &dVz);
+        R2[i] = R * R;
+        if (R2tap < R2[i]) {
+            double tap = cos(tap_cf * (R2[i] - R2tap));
+            double dtap = sin(tap_cf * (R2[i] - R2tap));
+            dVz = dVz * tap - tap_cf * Vz * dtap;
+            Vz = Vz * tap;
+        }
+        c0[i] = Vz;
+        c1[i] = dVz;
+    }
+    for (int i = 0; i < MS_NR - 1; i++) {
+        double idR = 1.0 / (R2[i + 1] - R2[i]);
+        double V = c0[i], Vn = c0[i + 1], dV = c1[i], dVn = c1[i + 1];
+        double m = (Vn - V) * idR;
+        double n = dV + dVn;
+        c2[i] = (3.0 * m - n - dV) * idR;
+        c3[i] = (n - 2.0 * m) * idR * idR;
+    }
+    c2[MS_NR - 1] = 0.0;
+    c3[MS_NR - 1] = 0.0;
+    if (rmax) *rmax = rmx;
+    return 0;
+}
+
+/* unrolledBinarySearch_c_nR + get_value_Cubic_Spline (basic_functions_dev.cuh:47-75) */
+static double or_spline_eval(const double* R2, const double* c0, const double* c1, const double* c2,
+                             const double* c3, double x)
+{
+    int i0 = 0, ie = MS_NR - 1;
+    for (int k = 0; k < 7; k++) {
+        int im = (i0 + ie) >> 1;
+        if (x < R2[im]) ie = im; else i0 = im;
+    }
+    double d = x - R2[i0];
+    return ((c3[i0] * d + c2[i0]) * d + c1[i0]) * d + c0[i0];
+}
+
+/* ------------------------------------------------------------------------ */
+/* common simulation context                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    double lambda, sigma, gamma, vr_factor;
+    int nx, ny;
+    long N;
+    double lx, ly, dx, dy;
+    float dgx_f, dgy_f;
+    double dgx, dgy;
+    double gl2, alpha;
+    double g0x, g0y;
+    double prop_w;
+} or_sim;
+
+static void or_sim_init(const ms_params* p, or_sim* s)
+{
+    or_physics(p->E0, &s->lambda, &s->sigma, &s->gamma);
+    s->vr_factor = s->sigma / cos(p->theta); /* get_Vr_factor(lambda, gamma, theta) */
+    s->nx = p->nx;
+    s->ny = p->ny;
+    s->N = (long)p->nx * p->ny;
+    s->lx = p->lx;
+    s->ly = p->ly;
+    s->dx = p->lx / p->nx;
+    s->dy = p->ly / p->ny;
+    s->dgx = 1.0 / p->lx;
+    s->dgy = 1.0 / p->ly;
+    s->dgx_f = 1.0f / (float)p->lx;
+    s->dgy_f = 1.0f / (float)p->ly;
+    /* Grid_2d_Dev::set_input_data (grid_dev.cuh:307-325) */
+    double gmax = fmin((p->nx / 2) * s->dgx, (p->ny / 2) * s->dgy);
+    double gl = 2.0 * gmax / 3.0;
+    s->gl2 = gl * gl;
+    s->alpha = log(1.0 / 1e-2 - 1.0) / ((gl + 0.25) * (gl + 0.25) - s->gl2);
+    /* gx_0 / gy_0 (multislice_params_dev.cuh:201-208) */
+    s->g0x = sin(p->theta) * cos(p->phi) / s->lambda;
+    s->g0y = sin(p->theta) * sin(p->phi) / s->lambda;
+    s->prop_w = -OR_PI * s->lambda * p->dz; /* propagator_factor * z (propagation_function.cuh:31, :49-57) */
+}
+
+static inline int or_fshift(int i, int n) { return i < n / 2 ? i : i - n; }
+
+/* float frequency squared, exactly as the engine computes it for masks */
+static inline float or_g2f(const or_sim* s, int ix, int iy)
+{
+    float gx = (float)or_fshift(ix, s->nx) * s->dgx_f;
+    float gy = (float)or_fshift(iy, s->ny) * s->dgy_f;
+    return gx * gx + gy * gy;
+}
+
+static float or_g2_thr(double ang, double lambda)
+{
+    float g = (float)(sin(ang) / lambda);
+    return g * g;
+}
+
+/* Lens_Dev coefficients (lens_dev.cuh:40-57); a term is dropped when its
+   coefficient is zero within the reference's float tolerance (nonZero_dev,
+   misc_dev.cuh:17-23, 1e-5 absolute). */
+typedef struct {
+    int m;
+    double cc10, cc12, cc21, cc23, cc30, cc32, cc34, cc41, cc43, cc45, cc50, cc52, cc54, cc56;
+    double p12, p21, p23, p32, p34, p41, p43, p45, p52, p54, p56;
+    float g2min, g2max;
+    int phi_req;
+} or_lens;
+
+static double or_gate(double v) { return fabs(v) > 1e-5 ? v : 0.0; }
+
+static void or_lens_init(const ms_lens* L, double lambda, double c10_shift, or_lens* o)
+{
+    double l = lambda, l2 = l * l, l3 = l2 * l, l4 = l3 * l, l5 = l4 * l;
+    o->m = L->m;
+    o->cc10 = or_gate(-OR_PI * (L->c10 + c10_shift) * l);
+    o->cc12 = or_gate(-OR_PI * L->c12 * l);
+    o->cc21 = or_gate(-2.0 * OR_PI * L->c21 * l2 / 3.0);
+    o->cc23 = or_gate(-2.0 * OR_PI * L->c23 * l2 / 3.0);
+    o->cc30 = or_gate(-OR_PI * L->c30 * l3 / 2.0);
+    o->cc32 = or_gate(-OR_PI * L->c32 * l3 / 2.0);
+    o->cc34 = or_gate(-OR_PI * L->c34 * l3 / 2.0);
+    o->cc41 = or_gate(-2.0 * OR_PI * L->c41 * l4 / 5.0);
+    o->cc43 = or_gate(-2.0 * OR_PI * L->c43 * l4 / 5.0);
+    o->cc45 = or_gate(-2.0 * OR_PI * L->c45 * l4 / 5.0);
+    o->cc50 = or_gate(-OR_PI * L->c50 * l5 / 3.0);
+    o->cc52 = or_gate(-OR_PI * L->c52 * l5 / 3.0);
+    o->cc54 = or_gate(-OR_PI * L->c54 * l5 / 3.0);
+    o->cc56 = or_gate(-OR_PI * L->c56 * l5 / 3.0);
+    o->p12 = L->phi12; o->p21 = L->phi21; o->p23 = L->phi23; o->p32 = L->phi32; o->p34 = L->phi34;
+    o->p41 = L->phi41; o->p43 = L->phi43; o->p45 = L->phi45; o->p52 = L->phi52; o->p54 = L->phi54;
+    o->p56 = L->phi56;
+    o->g2min = L->inner_aper_ang > 0 ? or_g2_thr(L->inner_aper_ang, lambda) : 0.0f;
+    o->g2max = L->outer_aper_ang > 0 ? or_g2_thr(L->outer_aper_ang, lambda) : FLT_MAX;
+    o->phi_req = (o->m != 0) || o->cc12 != 0 || o->cc21 != 0 || o->cc23 != 0 || o->cc32 != 0 ||
+                 o->cc34 != 0 || o->cc41 != 0 || o->cc43 != 0 || o->cc45 != 0 || o->cc52 != 0 ||
+                 o->cc54 != 0 || o->cc56 != 0;
+}
+
+/* coherent_phase_shift (basic_functions_dev.cuh:215-234) */
+static double or_chi(const or_lens* o, double gx, double gy)
+{
+    double g2 = gx * gx + gy * gy, g4 = g2 * g2, g6 = g4 * g2;
+    double chi = o->cc10 * g2 + o->cc30 * g4 + o->cc50 * g6;
+    if (o->phi_req) {
+        double g = sqrt(g2), g3 = g2 * g, g5 = g4 * g;
+        double ph = atan2(gy, gx);
+        if (fabs(ph) > 1e-5) chi += o->m * ph;
+        chi += o->cc12 * g2 * sin(2 * (ph - o->p12));
+        chi += o->cc21 * g3 * sin(ph - o->p21) + o->cc23 * g3 * sin(3 * (ph - o->p23));
+        chi += o->cc32 * g4 * sin(2 * (ph - o->p32)) + o->cc34 * g4 * sin(4 * (ph - o->p34));
+        chi += o->cc41 * g5 * sin(ph - o->p41) + o->cc43 * g5 * sin(3 * (ph - o->p43)) +
+               o->cc45 * g5 * sin(5 * (ph - o->p45));
+        chi += o->cc52 * g6 * sin(2 * (ph - o->p52)) + o->cc54 * g6 * sin(4 * (ph - o->p54)) +
+               o->cc56 * g6 * sin(6 * (ph - o->p56));
+    }
+    return chi;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FFT: iterative radix-2, unnormalised, sign -1 forward (CUFFT_FORWARD)      */
+/* ------------------------------------------------------------------------ */
+static void or_fft1(cplx* a, int n, int sign, const cplx* tw /* n/2 entries exp(-2 pi i k/n) */)
+{
+    for (int i = 1, j = 0; i < n; i++) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            cplx t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        int step = n / len;
+        for (int i = 0; i < n; i += len) {
+            for (int k = 0; k < len / 2; k++) {
+                cplx w = tw[k * step];
+                if (sign > 0) w = conj(w);
+                cplx u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+        }
+    }
+}
+
+static cplx* or_twiddles(int n)
+{
+    cplx* t = (cplx*)malloc(sizeof(cplx) * (size_t)(n / 2 > 0 ? n / 2 : 1));
+    for (int k = 0; k < n / 2; k++) {
+        double a = -2.0 * OR_PI * (double)k / (double)n;
+        t[k] = cos(a) + I * sin(a);
+    }
+    return t;
+}
+
+static void or_fft2c(cplx* d, int nx, int ny, int sign)
+{
+    cplx* twx = or_twiddles(nx);
+    cplx* twy = or_twiddles(ny);
+    int inpar = 0;
+#ifdef _OPENMP
+    inpar = omp_in_parallel();
+#endif
+    int nth = inpar ? 1 : or_get_threads();
+#pragma omp parallel for num_threads(nth) schedule(static)
+    for (int r = 0; r < ny; r++) or_fft1(d + (size_t)r * nx, nx, sign, twx);
+#pragma omp parallel num_threads(nth)
+    {
+        cplx* col = (cplx*)malloc(sizeof(cplx) * (size_t)ny);
+#pragma omp for schedule(static)
+        for (int c = 0; c < nx; c++) {
+            for (int r = 0; r < ny; r++) col[r] = d[(size_t)r * nx + c];
+            or_fft1(col, ny, sign, twy);
+            for (int r = 0; r < ny; r++) d[(size_t)r * nx + c] = col[r];
+        }
+        free(col);
+    }
+    free(twx);
+    free(twy);
+}
+
+void or_fft2(double* data, int nx, int ny, int sign) { or_fft2c((cplx*)data, nx, ny, sign); }
+
+/* ------------------------------------------------------------------------ */
+/* specimen of one configuration: displaced, sliced, grouped by slice        */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int ns;
+    float* bounds;
+    int64_t n;
+    float *x, *y, *z;
+    int* slice;
+    int64_t* order;    /* atom indices sorted by slice */
+    int64_t* start;    /* ns+1 offsets into order */
+    double z_init;     /* slice_middle_z(0) */
+} or_spec;
+
+static int or_spec_build(const ms_params* p, const ms_atoms* a, int conf, or_spec* sp)
+{
+    memset(sp, 0, sizeof(*sp));
+    sp->n = a->n;
+    sp->x = (float*)malloc(sizeof(float) * (size_t)(a->n + 1));
+    sp->y = (float*)malloc(sizeof(float) * (size_t)(a->n + 1));
+    sp->z = (float*)malloc(sizeof(float) * (size_t)(a->n + 1));
+    sp->slice = (int*)malloc(sizeof(int) * (size_t)(a->n + 1));
+    or_displace(p, a, conf, sp->x, sp->y, sp->z);
+    int ns = or_slices(p, sp->z, a->n, NULL, 0, NULL);
+    sp->ns = ns;
+    sp->bounds = (float*)malloc(sizeof(float) * (size_t)(ns + 1));
+    or_slices(p, sp->z, a->n, sp->bounds, ns + 1, sp->slice);
+    sp->start = (int64_t*)calloc((size_t)ns + 2, sizeof(int64_t));
+    sp->order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(a->n + 1));
+    for (int64_t i = 0; i < a->n; i++)
+        if (sp->slice[i] >= 0) sp->start[sp->slice[i] + 1]++;
+    for (int s = 0; s < ns; s++) sp->start[s + 1] += sp->start[s];
+    int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)(ns + 1));
+    for (int s = 0; s <= ns; s++) fill[s] = sp->start[s];
+    for (int64_t i = 0; i < a->n; i++)
+        if (sp->slice[i] >= 0) sp->order[fill[sp->slice[i]]++] = i;
+    free(fill);
+    /* Slice::z_m (slice.hpp:19-22) */
+    sp->z_init = ns > 0 ? (double)(float)(0.5 * (double)(sp->bounds[1] + sp->bounds[0])) : 0.0;
+    return ns;
+}
+
+static void or_spec_free(or_spec* sp)
+{
+    free(sp->bounds);
+    free(sp->x);
+    free(sp->y);
+    free(sp->z);
+    free(sp->slice);
+    free(sp->order);
+    free(sp->start);
+}
+
+/* element spline cache */
+typedef struct {
+    int Z;
+    double R2[MS_NR], c0[MS_NR], c1[MS_NR], c2[MS_NR], c3[MS_NR];
+    double rmax;
+} or_elem;
+
+typedef struct {
+    int n;
+    or_elem e[128];
+} or_elems;
+
+static or_elem* or_elem_get(const ms_params* p, or_elems* es, int Z)
+{
+    for (int i = 0; i < es->n; i++)
+        if (es->e[i].Z == Z) return &es->e[i];
+    or_elem* e = &es->e[es->n++];
+    e->Z = Z;
+    or_spline(p, Z, e->R2, e->c0, e->c1, e->c2, e->c3, &e->rmax);
+    return e;
+}
+
+/* generate_potential_single_slice: gen_slice_potential_kernel
+   (device_kernels.cuh:28-47) with coeff = Vr_factor; each atom adds
+   occ * spline(R^2) to every pixel with R^2 < R_max^2. */
+static void or_slice_potential(const ms_params* p, const ms_atoms* a, const or_sim* s, const or_spec* sp,
+                               or_elems* es, int islice, double* V)
+{
+    memset(V, 0, sizeof(double) * (size_t)s->N);
+    if (islice < 0 || islice >= sp->ns) return;
+    for (int64_t k = sp->start[islice]; k < sp->start[islice + 1]; k++) {
+        int64_t ia = sp->order[k];
+        or_elem* e = or_elem_get(p, es, a->Z[ia]);
+        double xa = sp->x[ia], ya = sp->y[ia];
+        double rmax2 = e->rmax * e->rmax;
+        double coeff = s->vr_factor * (double)a->occ[ia];
+        int ix0 = (int)floor((xa - e->rmax) / s->dx) - 1, ix1 = (int)ceil((xa + e->rmax) / s->dx) + 1;
+        int iy0 = (int)floor((ya - e->rmax) / s->dy) - 1, iy1 = (int)ceil((ya + e->rmax) / s->dy) + 1;
+        for (int iy = iy0; iy <= iy1; iy++) {
+            int ry;
+            if (p->pot_wrap) ry = ((iy % s->ny) + s->ny) % s->ny;
+            else {
+                if (iy < 0 || iy >= s->ny) continue;
+                ry = iy;
+            }
+            double dyp = iy * s->dy - ya;
+            for (int ix = ix0; ix <= ix1; ix++) {
+                int rx;
+                if (p->pot_wrap) rx = ((ix % s->nx) + s->nx) % s->nx;
+                else {
+                    if (ix < 0 || ix >= s->nx) continue;
+                    rx = ix;
+                }
+                double dxp = ix * s->dx - xa;
+                double R2 = dxp * dxp + dyp * dyp;
+                if (R2 < rmax2) V[(size_t)ry * s->nx + rx] += coeff * or_spline_eval(e->R2, e->c0, e->c1, e->c2, e->c3, R2);
+            }
+        }
+    }
+}
+
+int or_potential(const ms_params* p, const ms_atoms* a, int conf, double* V, int64_t cap, int* n_slices,
+                 double* z_init)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    or_spec sp;
+    or_spec_build(p, a, conf, &sp);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    if (n_slices) *n_slices = sp.ns;
+    if (z_init) *z_init = sp.z_init;
+    int rc = 0;
+    if (V) {
+        if ((int64_t)sp.ns * s.N > cap) rc = 1;
+        else
+            for (int i = 0; i < sp.ns; i++) or_slice_potential(p, a, &s, &sp, es, i, V + (size_t)i * s.N);
+    }
+    free(es);
+    or_spec_free(&sp);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* operators on a wave                                                       */
+/* ------------------------------------------------------------------------ */
+/* Propagator table P(k) (gen_propagator_kernel, device_kernels.cuh:215-234) */
+static void or_propagator(const ms_params* p, const or_sim* s, cplx* P)
+{
+    for (int iy = 0; iy < s->ny; iy++)
+        for (int ix = 0; ix < s->nx; ix++) {
+            size_t k = (size_t)iy * s->nx + ix;
+            if (p->dz == 0.0) {
+                P[k] = 1.0;
+                continue;
+            }
+            double gx = or_fshift(ix, s->nx) * s->dgx, gy = or_fshift(iy, s->ny) * s->dgy;
+            double amp = 1.0 / (double)s->N;
+            if (p->bwl) amp *= 1.0 / (1.0 + exp(s->alpha * (gx * gx + gy * gy - s->gl2)));
+            double th = s->prop_w * ((gx - s->g0x) * (gx - s->g0x) + (gy - s->g0y) * (gy - s->g0y));
+            P[k] = amp * (cos(th) + I * sin(th));
+        }
+}
+
+/* k-space probe (Generate_probe, device_kernels.cuh:363-388) */
+static void or_probe_k(const or_sim* s, const or_lens* L, double px, double py, cplx* W)
+{
+    double xf = -2.0 * OR_PI * px, yf = -2.0 * OR_PI * py; /* exp_factor_*_pos with x_b - L/2 = position */
+    for (int iy = 0; iy < s->ny; iy++)
+        for (int ix = 0; ix < s->nx; ix++) {
+            size_t k = (size_t)iy * s->nx + ix;
+            float g2 = or_g2f(s, ix, iy);
+            if (L->g2min <= g2 && g2 < L->g2max) {
+                double gx = or_fshift(ix, s->nx) * s->dgx, gy = or_fshift(iy, s->ny) * s->dgy;
+                double ph = or_chi(L, gx, gy) + xf * gx + yf * gy;
+                W[k] = cos(ph) + I * sin(ph);
+            } else
+                W[k] = 0.0;
+        }
+}
+
+/* incident wave (Incident_Wave::generate_incident_beam, incident_wave.cuh:29-46) */
+static void or_incident(const ms_params* p, const or_sim* s, double px, double py, double z_init, cplx* w)
+{
+    int iw = p->iw_type;
+    if (iw < 0) iw = (p->simulation_type == MS_SIM_HRTEM || p->simulation_type == MS_SIM_ED) ? MS_IW_PLANE : MS_IW_CONVERGENT;
+    if (iw == MS_IW_CONVERGENT) {
+        or_lens L;
+        or_lens_init(&p->cond_lens, s->lambda, z_init, &L);
+        or_probe_k(s, &L, px, py, w);
+        or_fft2c(w, s->nx, s->ny, +1);
+    } else {
+        for (long k = 0; k < s->N; k++) w[k] = 1.0;
+    }
+}
+
+/* wave_modulation (wave_function.cuh:60-73): for every slice but the last,
+   transmit (forward FFT of t*psi, fftcallbacks.cuh:36-49) then propagate
+   (inverse FFT of P*Psi, fftcallbacks.cuh:11-22); the last slice only
+   transmits, leaving the exit wave in reciprocal space. */
+static void or_transmit(cplx* w, const double* V, long N)
+{
+    for (long k = 0; k < N; k++) w[k] *= cos(V[k]) + I * sin(V[k]);
+}
+
+static void or_multislice(const or_sim* s, cplx* w, const double* Vall, int ns, const cplx* P,
+                          const ms_params* p, const ms_atoms* a, const or_spec* sp, or_elems* es, double* Vtmp)
+{
+    for (int i = 0; i < ns; i++) {
+        const double* V = Vall ? Vall + (size_t)i * s->N : NULL;
+        if (!V) {
+            or_slice_potential(p, a, s, sp, es, i, Vtmp);
+            V = Vtmp;
+        }
+        or_transmit(w, V, s->N);
+        or_fft2c(w, s->nx, s->ny, -1);
+        if (i < ns - 1) {
+            for (long k = 0; k < s->N; k++) w[k] *= P[k];
+            or_fft2c(w, s->nx, s->ny, +1);
+        }
+    }
+}
+
+/* fft_shift (device_kernels.cuh:342-362) on a real image */
+static void or_fftshift(double* img, int nx, int ny)
+{
+    double* t = (double*)malloc(sizeof(double) * (size_t)nx * ny);
+    for (int iy = 0; iy < ny; iy++)
+        for (int ix = 0; ix < nx; ix++)
+            t[(size_t)((iy + ny / 2) % ny) * nx + (ix + nx / 2) % nx] = img[(size_t)iy * nx + ix];
+    memcpy(img, t, sizeof(double) * (size_t)nx * ny);
+    free(t);
+}
+
+static void or_confs(const ms_params* p, int* c0, int* c1, double* w)
+{
+    if (p->phonon_model == MS_PHONON_FROZEN && p->pn_nconf > 0) {
+        *c0 = 1;
+        *c1 = p->pn_nconf;
+        *w = 1.0 / (double)p->pn_nconf; /* get_weight (multislice_params_dev.cuh:209-216) */
+    } else {
+        *c0 = 0;
+        *c1 = 0;
+        *w = 1.0;
+    }
+}
+
+/* ED_HRTEM (single_simulator.cuh:11-126) and CBED_CBEI (:128-206) */
+static int or_tem_like(const ms_params* p, const ms_atoms* a, double* img, double* re, double* im, int kspace)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    int c0, c1;
+    double w;
+    or_confs(p, &c0, &c1, &w);
+    int full = p->data_record == MS_RECORD_WAVE;
+    if (img) memset(img, 0, sizeof(double) * (size_t)s.N);
+    if (re) memset(re, 0, sizeof(double) * (size_t)s.N);
+    if (im) memset(im, 0, sizeof(double) * (size_t)s.N);
+    cplx* wv = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    double* Vt = (double*)malloc(sizeof(double) * (size_t)s.N);
+    or_propagator(p, &s, P);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    for (int c = c0; c <= c1; c++) {
+        or_spec sp;
+        or_spec_build(p, a, c, &sp);
+        or_incident(p, &s, p->iw_x, p->iw_y, sp.z_init, wv);
+        or_multislice(&s, wv, NULL, sp.ns, P, p, a, &sp, es, Vt);
+        if (!kspace) {
+            /* OL_modulation -> CTF_TEM (lens_modulation.cuh:78-89): apply_CTF_kernel, inverse FFT */
+            or_lens L;
+            or_lens_init(&p->obj_lens, s.lambda, 0.0, &L);
+            for (int iy = 0; iy < s.ny; iy++)
+                for (int ix = 0; ix < s.nx; ix++) {
+                    size_t k = (size_t)iy * s.nx + ix;
+                    float g2 = or_g2f(&s, ix, iy);
+                    if (L.g2min <= g2 && g2 < L.g2max) {
+                        double gx = or_fshift(ix, s.nx) * s.dgx, gy = or_fshift(iy, s.ny) * s.dgy;
+                        double ch = or_chi(&L, gx, gy);
+                        wv[k] *= cos(ch) + I * sin(ch);
+                    } else
+                        wv[k] = 0.0;
+                }
+            or_fft2c(wv, s.nx, s.ny, +1);
+        }
+        for (long k = 0; k < s.N; k++) {
+            if (full) {
+                re[k] += w * creal(wv[k]);
+                im[k] += w * cimag(wv[k]);
+            } else
+                img[k] += w * (creal(wv[k]) * creal(wv[k]) + cimag(wv[k]) * cimag(wv[k]));
+        }
+        or_spec_free(&sp);
+    }
+    if (kspace) {
+        if (full) {
+            or_fftshift(re, s.nx, s.ny);
+            or_fftshift(im, s.nx, s.ny);
+        } else
+            or_fftshift(img, s.nx, s.ny);
+    }
+    free(es);
+    free(wv);
+    free(P);
+    free(Vt);
+    return 0;
+}
+
+int or_simulate_tem(const ms_params* p, const ms_atoms* a, double* img, double* re, double* im)
+{
+    return or_tem_like(p, a, img, re, im, p->simulation_type != MS_SIM_HRTEM);
+}
+
+int or_simulate_cbed(const ms_params* p, const ms_atoms* a, double* img, double* re, double* im)
+{
+    return or_tem_like(p, a, img, re, im, 1);
+}
+
+/* detector sums (sum_square_over_Det, device_kernels.cuh:534-579) */
+static void or_detect(const ms_params* p, const or_sim* s, const cplx* W, double* out)
+{
+    float g2i[MS_MAX_DET], g2o[MS_MAX_DET];
+    for (int d = 0; d < p->n_det; d++) {
+        g2i[d] = or_g2_thr(p->det_inner[d], s->lambda);
+        g2o[d] = or_g2_thr(p->det_outer[d], s->lambda);
+        out[d] = 0.0;
+    }
+    for (int iy = 0; iy < s->ny; iy++)
+        for (int ix = 0; ix < s->nx; ix++) {
+            size_t k = (size_t)iy * s->nx + ix;
+            float g2 = or_g2f(s, ix, iy);
+            double a2 = creal(W[k]) * creal(W[k]) + cimag(W[k]) * cimag(W[k]);
+            for (int d = 0; d < p->n_det; d++)
+                if (g2i[d] <= g2 && g2 <= g2o[d]) out[d] += a2;
+        }
+}
+
+/* run_STEM_tile_simu (scan_simulator.cuh:11-113) for a grid that covers the
+   specimen: per configuration, store all slice potentials, then run every
+   probe position and integrate each detector. */
+int or_simulate_stem(const ms_params* p, const ms_atoms* a, double* stem)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    int c0, c1;
+    double w;
+    or_confs(p, &c0, &c1, &w);
+    int npos = p->scan_nx * p->scan_ny;
+    memset(stem, 0, sizeof(double) * (size_t)p->n_det * npos);
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    or_propagator(p, &s, P);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    for (int c = c0; c <= c1; c++) {
+        or_spec sp;
+        or_spec_build(p, a, c, &sp);
+        double* V = (double*)malloc(sizeof(double) * (size_t)s.N * (sp.ns > 0 ? sp.ns : 1));
+        for (int i = 0; i < sp.ns; i++) or_slice_potential(p, a, &s, &sp, es, i, V + (size_t)i * s.N);
+        int nth = or_get_threads();
+#pragma omp parallel num_threads(nth)
+        {
+            cplx* wv = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+            double Id[MS_MAX_DET];
+#pragma omp for schedule(dynamic, 1)
+            for (int ip = 0; ip < npos; ip++) {
+                int ix = ip % p->scan_nx, iy = ip / p->scan_nx;
+                double px = p->scan_x0 + ix * p->scan_dx, py = p->scan_y0 + iy * p->scan_dy;
+                or_incident(p, &s, px, py, sp.z_init, wv);
+                or_multislice(&s, wv, V, sp.ns, P, p, a, &sp, es, NULL);
+                or_detect(p, &s, wv, Id);
+                for (int d = 0; d < p->n_det; d++) stem[(size_t)d * npos + ip] += w * Id[d];
+            }
+            free(wv);
+        }
+        free(V);
+        or_spec_free(&sp);
+    }
+    free(es);
+    free(P);
+    return 0;
+}
+
+/* run_thickness_simu (thickness_simulator.cuh:11-85), with the transmission
+   the reference forgets to attach in this path applied: after each slice
+   (transmit + propagate) the wave is filtered by the annulus of detector
+   `thick_det` (Filter_wave, device_kernels.cuh:389-410) and its intensity
+   recorded.  Frames follow the static specimen's slice count; a phonon
+   configuration with fewer slices continues through empty slices. */
+int or_simulate_thickness(const ms_params* p, const ms_atoms* a, double* frames, int64_t cap, int* n_frames)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    int c0, c1;
+    double w;
+    or_confs(p, &c0, &c1, &w);
+    or_spec sp0;
+    or_spec_build(p, a, 0, &sp0);
+    int nf = sp0.ns;
+    or_spec_free(&sp0);
+    if (n_frames) *n_frames = nf;
+    if (!frames) return 0;
+    if ((int64_t)nf * s.N > cap) return 1;
+    memset(frames, 0, sizeof(double) * (size_t)nf * s.N);
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    or_propagator(p, &s, P);
+    cplx* wv = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    cplx* tmp = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    double* V = (double*)malloc(sizeof(double) * (size_t)s.N);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    int d = p->thick_det;
+    float g2i = or_g2_thr(p->det_inner[d], s.lambda), g2o = or_g2_thr(p->det_outer[d], s.lambda);
+    for (int c = c0; c <= c1; c++) {
+        or_spec sp;
+        or_spec_build(p, a, c, &sp);
+        or_incident(p, &s, p->iw_x, p->iw_y, sp.z_init, wv);
+        for (int i = 0; i < nf; i++) {
+            or_slice_potential(p, a, &s, &sp, es, i, V);
+            or_transmit(wv, V, s.N);
+            or_fft2c(wv, s.nx, s.ny, -1);
+            for (long k = 0; k < s.N; k++) wv[k] *= P[k];
+            or_fft2c(wv, s.nx, s.ny, +1);
+            memcpy(tmp, wv, sizeof(cplx) * (size_t)s.N);
+            or_fft2c(tmp, s.nx, s.ny, -1);
+            for (int iy = 0; iy < s.ny; iy++)
+                for (int ix = 0; ix < s.nx; ix++) {
+                    size_t k = (size_t)iy * s.nx + ix;
+                    float g2 = or_g2f(&s, ix, iy);
+                    if (g2i <= g2 && g2 <= g2o) tmp[k] *= 1.0 / (double)s.N;
+                    else tmp[k] = 0.0;
+                }
+            or_fft2c(tmp, s.nx, s.ny, +1);
+            double* f = frames + (size_t)i * s.N;
+            for (long k = 0; k < s.N; k++) f[k] += w * (creal(tmp[k]) * creal(tmp[k]) + cimag(tmp[k]) * cimag(tmp[k]));
+        }
+        or_spec_free(&sp);
+    }
+    free(es);
+    free(V);
+    free(tmp);
+    free(wv);
+    free(P);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* raw STEM forward and its adjoint on caller phase arrays                   */
+/* ------------------------------------------------------------------------ */
+static void or_exp_phase(const float* V, long N, cplx* t)
+{
+    for (long k = 0; k < N; k++) t[k] = cos((double)V[k]) + I * sin((double)V[k]);
+}
+
+int or_stem_forward_potential(const ms_params* p, const float* V, int n_slices, double z_init,
+                              const double* probe_xy, int n_probe, double* Iout)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    or_propagator(p, &s, P);
+    int nth = or_get_threads();
+#pragma omp parallel num_threads(nth)
+    {
+        cplx* wv = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+        double* Vd = (double*)malloc(sizeof(double) * (size_t)s.N);
+#pragma omp for schedule(dynamic, 1)
+        for (int ip = 0; ip < n_probe; ip++) {
+            ms_params q = *p;
+            q.iw_type = MS_IW_CONVERGENT;
+            or_incident(&q, &s, probe_xy[2 * ip], probe_xy[2 * ip + 1], z_init, wv);
+            for (int i = 0; i < n_slices; i++) {
+                for (long k = 0; k < s.N; k++) Vd[k] = V[(size_t)i * s.N + k];
+                or_transmit(wv, Vd, s.N);
+                or_fft2c(wv, s.nx, s.ny, -1);
+                if (i < n_slices - 1) {
+                    for (long k = 0; k < s.N; k++) wv[k] *= P[k];
+                    or_fft2c(wv, s.nx, s.ny, +1);
+                }
+            }
+            or_detect(p, &s, wv, Iout + (size_t)ip * p->n_det);
+        }
+        free(wv);
+        free(Vd);
+    }
+    free(P);
+    return 0;
+}
+
+/* Adjoint: with D the unnormalised forward DFT, the forward chain is
+   psi_0 = D^H Psi0, x_s = t_s psi_s, psi_{s+1} = D^H (P . D x_s), Psi = D x_{S-1}.
+   For L = sum_d (I_d - T_d)^2 the backward chain is
+   lambda = sum_d 4 (I_d - T_d) Psi [k in d],   mu = D^H lambda,
+   dL/dV_s = Re(i t_s psi_s conj(xbar_s)),      nu_s = conj(t_s) xbar_s,
+   xbar_{s} = D^H (conj(P) . D nu_{s+1}),       Psi0bar = D nu_0,
+   dL/dC = sum chi_C Re(i Psi0 conj(Psi0bar)). */
+int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_init, const double* probe_xy,
+                     int n_probe, const float* target, double* loss, double* dL_dV, double* dL_dC10,
+                     double* dL_dC30)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    long N = s.N;
+    int S = n_slices;
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+    or_propagator(p, &s, P);
+    cplx* T = (cplx*)malloc(sizeof(cplx) * (size_t)N * S);
+    for (int i = 0; i < S; i++) or_exp_phase(V + (size_t)i * N, N, T + (size_t)i * N);
+    memset(dL_dV, 0, sizeof(double) * (size_t)N * S);
+    double Ltot = 0.0, g10 = 0.0, g30 = 0.0;
+    or_lens L;
+    or_lens_init(&p->cond_lens, s.lambda, z_init, &L);
+    float g2i[MS_MAX_DET], g2o[MS_MAX_DET];
+    for (int d = 0; d < p->n_det; d++) {
+        g2i[d] = or_g2_thr(p->det_inner[d], s.lambda);
+        g2o[d] = or_g2_thr(p->det_outer[d], s.lambda);
+    }
+    int nth = or_get_threads();
+    double* gV_all = (double*)calloc((size_t)nth * N * S, sizeof(double));
+    double Lp[1024] = {0}, a10p[1024] = {0}, a30p[1024] = {0};
+    if (nth > 1024) nth = 1024;
+#pragma omp parallel num_threads(nth)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double* gV = gV_all + (size_t)tid * N * S;
+        cplx* psi = (cplx*)malloc(sizeof(cplx) * (size_t)N * S);
+        cplx* W0 = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+        cplx* w = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+#pragma omp for schedule(dynamic, 1)
+        for (int ip = 0; ip < n_probe; ip++) {
+            or_probe_k(&s, &L, probe_xy[2 * ip], probe_xy[2 * ip + 1], W0);
+            memcpy(w, W0, sizeof(cplx) * (size_t)N);
+            or_fft2c(w, s.nx, s.ny, +1);
+            for (int i = 0; i < S; i++) {
+                memcpy(psi + (size_t)i * N, w, sizeof(cplx) * (size_t)N);
+                const cplx* t = T + (size_t)i * N;
+                for (long k = 0; k < N; k++) w[k] *= t[k];
+                or_fft2c(w, s.nx, s.ny, -1);
+                if (i < S - 1) {
+                    for (long k = 0; k < N; k++) w[k] *= P[k];
+                    or_fft2c(w, s.nx, s.ny, +1);
+                }
+            }
+            double Id[MS_MAX_DET];
+            or_detect(p, &s, w, Id);
+            double r[MS_MAX_DET];
+            for (int d = 0; d < p->n_det; d++) {
+                r[d] = Id[d] - (double)target[(size_t)ip * p->n_det + d];
+                Lp[tid] += r[d] * r[d];
+            }
+            for (int iy = 0; iy < s.ny; iy++)
+                for (int ix = 0; ix < s.nx; ix++) {
+                    size_t k = (size_t)iy * s.nx + ix;
+                    float g2 = or_g2f(&s, ix, iy);
+                    double f = 0.0;
+                    for (int d = 0; d < p->n_det; d++)
+                        if (g2i[d] <= g2 && g2 <= g2o[d]) f += 4.0 * r[d];
+                    w[k] *= f;
+                }
+            or_fft2c(w, s.nx, s.ny, +1); /* mu = xbar_{S-1} */
+            for (int i = S - 1; i >= 0; i--) {
+                if (i < S - 1) {
+                    or_fft2c(w, s.nx, s.ny, -1);
+                    for (long k = 0; k < N; k++) w[k] *= conj(P[k]);
+                    or_fft2c(w, s.nx, s.ny, +1);
+                }
+                const cplx* t = T + (size_t)i * N;
+                const cplx* ps = psi + (size_t)i * N;
+                double* g = gV + (size_t)i * N;
+                for (long k = 0; k < N; k++) {
+                    g[k] += creal(I * t[k] * ps[k] * conj(w[k]));
+                    w[k] *= conj(t[k]);
+                }
+            }
+            or_fft2c(w, s.nx, s.ny, -1); /* Psi0bar */
+            for (int iy = 0; iy < s.ny; iy++)
+                for (int ix = 0; ix < s.nx; ix++) {
+                    size_t k = (size_t)iy * s.nx + ix;
+                    if (W0[k] == 0.0) continue;
+                    double gx = or_fshift(ix, s.nx) * s.dgx, gy = or_fshift(iy, s.ny) * s.dgy;
+                    double g2 = gx * gx + gy * gy;
+                    double q = creal(I * W0[k] * conj(w[k]));
+                    a10p[tid] += -OR_PI * s.lambda * g2 * q;
+                    a30p[tid] += -OR_PI * s.lambda * s.lambda * s.lambda * g2 * g2 / 2.0 * q;
+                }
+        }
+        free(psi);
+        free(W0);
+        free(w);
+    }
+    for (int t = 0; t < nth; t++) {
+        Ltot += Lp[t];
+        g10 += a10p[t];
+        g30 += a30p[t];
+        const double* gV = gV_all + (size_t)t * N * S;
+        for (long k = 0; k < N * S; k++) dL_dV[k] += gV[k];
+    }
+    free(gV_all);
+    *loss = Ltot;
+    *dL_dC10 = g10;
+    *dL_dC30 = g30;
+    free(T);
+    free(P);
+    return 0;
+}

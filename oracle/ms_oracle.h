@@ -1,0 +1,71 @@
+/*
+ * ms_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * FP64 CPU restatement of cudaEM's multislice operators.  It exists to
+ * check the CUDA engine; nothing in the shipped library links, loads or
+ * calls it.  Only tests/, __graft_entry__.smoke() and the cpu_baseline leg
+ * of bench.py use it.
+ *
+ * Parity status: the reference publishes no golden vectors and its source
+ * cannot be built as shipped (eleven headers are missing), so agreement
+ * with the reference's own outputs is pinned only through the
+ * reference-kernel shim under oracle/ref_shim/ (the reference's device
+ * kernels compiled with a small constants header) where that run exists;
+ * otherwise parity with the reference is unpinned and rests on the
+ * file:line restatement below plus physics invariants.
+ */
+#ifndef MS_ORACLE_H
+#define MS_ORACLE_H
+#include <stdint.h>
+#include "../include/cudaem_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* physics */
+void or_physics(double E0_kV, double* lambda, double* sigma, double* gamma);
+
+/* deterministic Gaussian pair keyed by (seed, conf, atom, stream) */
+double or_det_log(double s);
+void or_gauss_pair(uint64_t seed, int conf, int64_t atom, int stream, double* g0, double* g1);
+void or_displace(const ms_params* p, const ms_atoms* a, int conf, float* x, float* y, float* z);
+
+/* slicing on float z: returns the number of slices, fills bounds (n+1) and atom_slice */
+int or_slices(const ms_params* p, const float* z, int64_t n, float* bounds, int cap, int* atom_slice);
+
+/* radial spline of one element (FP64): R2, c0..c3 with MS_NR entries each */
+int or_spline(const ms_params* p, int Z, double* R2, double* c0, double* c1, double* c2, double* c3,
+              double* rmax);
+/* projected potential V_z(R) and dV_z/dR^2 of one element (before tapering) */
+int or_projected(const ms_params* p, int Z, double R, double* Vz, double* dVz_dR2);
+
+/* sigma-scaled projected potentials of configuration conf: V[n_slices][ny][nx] (rad) */
+int or_potential(const ms_params* p, const ms_atoms* a, int conf, double* V, int64_t cap,
+                 int* n_slices, double* z_init);
+
+/* unnormalised 2-D FFT, sign -1 forward, +1 inverse; data interleaved re,im */
+void or_fft2(double* data, int nx, int ny, int sign);
+
+/* simulators: outputs in double, same layouts as ms_output */
+int or_simulate_tem(const ms_params* p, const ms_atoms* a, double* img, double* re, double* im);
+int or_simulate_cbed(const ms_params* p, const ms_atoms* a, double* img, double* re, double* im);
+int or_simulate_stem(const ms_params* p, const ms_atoms* a, double* stem);
+int or_simulate_thickness(const ms_params* p, const ms_atoms* a, double* frames, int64_t cap,
+                          int* n_frames);
+
+/* raw STEM forward / adjoint on caller phase arrays V[n_slices][ny][nx] */
+int or_stem_forward_potential(const ms_params* p, const float* V, int n_slices, double z_init,
+                              const double* probe_xy, int n_probe, double* I);
+int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_init,
+                     const double* probe_xy, int n_probe, const float* target, double* loss,
+                     double* dL_dV, double* dL_dC10, double* dL_dC30);
+
+/* number of OpenMP threads the oracle uses (0 = runtime default) */
+void or_set_threads(int n);
+int or_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
