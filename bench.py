@@ -48,15 +48,18 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cbed", choices=["cbed", "stem", "hrtem"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
+    ap.add_argument("--nconf", type=int, default=0, help="phonon configurations (0: the workload's)")
     return ap.parse_args()
 
 
-def workload(config: str, rank: int = 0):
+def workload(config: str, rank: int = 0, cells_z: int = 0, nconf: int = 0):
     from cudaem_b200 import workloads as wl
     if config == "cbed":
-        p, at = wl.cbed_si()
+        cz = cells_z or 60
+        p, at = wl.cbed_si(cells=(16, 16, cz), nconf=nconf or 8)
         p.pn_seed = 42 + 1000 * rank
-        units = p.pn_nconf * 240
+        units = p.pn_nconf * 4 * cz
         desc = {"workload": "CBED Si[001] 16x16x60 cells, 1024^2, 240 slices x 1.358 A, 300 kV, 20 mrad, "
                             "8 frozen-phonon configurations per call", "grid": 1024, "slices": 240,
                 "phonon_configs": 8, "waves_per_potential": 1}
@@ -213,7 +216,9 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    p, at, units, desc = workload(args.config, rank)
+    p, at, units, desc = workload(args.config, rank, args.cells_z, args.nconf)
+    if args.cells_z or args.nconf:
+        desc = dict(desc, workload=desc["workload"] + f" [reduced: cells_z={args.cells_z}, nconf={args.nconf}]")
     ctx = cb.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
