@@ -139,6 +139,8 @@ PROTOTYPES = {
                                          C.c_int64, C.c_int, _P(C.c_int)]),
     "ms_stem_forward_potential": (C.c_int, [C.c_void_p, _P(ms_params), _P(C.c_float), C.c_int, C.c_int,
                                             C.c_double, _P(C.c_double), C.c_int, _P(C.c_float)]),
+    "ms_stem_forward_potential_noalloc": (C.c_int, [C.c_void_p, _P(ms_params), C.c_void_p, C.c_int, C.c_double,
+                                                    _P(C.c_double), C.c_int, C.c_void_p]),
     "ms_stem_backward": (C.c_int, [C.c_void_p, _P(ms_params), _P(C.c_float), C.c_int, C.c_int, C.c_double,
                                    _P(C.c_double), C.c_int, _P(C.c_float), _P(C.c_double), _P(C.c_float),
                                    _P(C.c_double), _P(C.c_double)]),

@@ -22,7 +22,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "engine.cu"]
+CU_SOURCES = ["kernels.cu", "engine.cu", "noalloc.cu"]
 CPP_SOURCES = ["host.cpp", "abi.cpp"]
 
 

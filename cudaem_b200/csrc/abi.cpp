@@ -282,6 +282,15 @@ ms_status ms_stem_forward_potential(ms_ctx* c, const ms_params* p, const float* 
     });
 }
 
+ms_status ms_stem_forward_potential_noalloc(void* stream, const ms_params* p, const float* V, int n_slices,
+                                            double z_init, const double* probe_xy, int n_probe, float* I)
+{
+    return guarded(nullptr, [&] {
+        MS_REQUIRE(p, MS_ERR_INVALID_ARG, "params is NULL");
+        msb::stem_forward_noalloc((cudaStream_t)stream, *p, V, n_slices, z_init, probe_xy, n_probe, I);
+    });
+}
+
 ms_status ms_stem_backward(ms_ctx* c, const ms_params* p, const float* V, int n_slices, int on_dev, double z_init,
                            const double* probe_xy, int n_probe, const float* target, double* loss, float* dL_dV,
                            double* dL_dC10, double* dL_dC30)

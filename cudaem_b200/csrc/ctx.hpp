@@ -54,4 +54,7 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
                        const double* xy, int np, const float* target, double* loss, float* dV, double* dC10,
                        double* dC30);
 void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_output* outs, double* lat);
+void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, int S, double z_init, const double* xy,
+                          int np, float* I);
+size_t noalloc_scratch_bytes();
 }  // namespace msb

@@ -1,0 +1,227 @@
+// STEM forward pass on caller potentials that allocates no device memory.
+//
+// Some callers cannot let a library call cudaMalloc: a host application whose
+// memory manager owns every device allocation (a framework plugin that must
+// stay inside its pool), a real-time acquisition loop that forbids the
+// implicit synchronisation cudaMalloc/cudaFree bring, or a process that has
+// already handed nearly all device memory to a pre-sized arena.  For them
+// this file runs the same fused slice passes as ms_stem_forward_potential,
+// but every scratch buffer it needs -- the probe-batch wave, the FFT
+// twiddles, the propagator factors, the wave table and the detector partial
+// sums -- lives in one file-scope __device__ array of fixed size.  The
+// caller provides the potentials and the output in its own device memory.
+//
+// The array is created when the library's module for this file is loaded on
+// a device and stays until the process exits (about 34 MiB per GPU).  Its
+// device address is looked up once per device, on the first call made with
+// that device current; that first call should therefore come before any
+// stream capture.  Every call shares the one array, so calls that overlap on
+// the GPU (different streams, or host threads) race on it and must be
+// serialised by the caller.  Nothing in the array needs to start at zero:
+// each call writes every value before reading it.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "engine.hpp"
+#include "fft_layout.hpp"
+#include "kernels.cuh"
+
+namespace msb {
+
+namespace {
+constexpr size_t kWaveBytes = size_t(32) << 20;       // probe-batch waves: nx*ny*8*batch <= 32 MiB
+constexpr int kMaxBatch = 256;
+constexpr int kMaxN = 2048;
+constexpr int kMaxBlk = 64;
+constexpr size_t kTableBytes = sizeof(float2) * 4 * kMaxN;                             // tw_x, tw_y, prop_x, prop_y
+constexpr size_t kWaveInfoBytes = sizeof(WaveInfo) * kMaxBatch;
+constexpr size_t kThrBytes = 256;                                                     // 2 * MS_MAX_DET floats
+constexpr size_t kIwaveBytes = sizeof(double) * kMaxBatch * MS_MAX_DET;
+constexpr size_t kPartialBytes = sizeof(double) * kMaxBatch * kMaxBlk * MS_MAX_DET;
+constexpr size_t kOffTables = 0;
+constexpr size_t kOffWaveInfo = kOffTables + kTableBytes;
+constexpr size_t kOffThr = kOffWaveInfo + kWaveInfoBytes;
+constexpr size_t kOffIwave = kOffThr + kThrBytes;
+constexpr size_t kOffPartial = kOffIwave + kIwaveBytes;
+constexpr size_t kOffWave = (kOffPartial + kPartialBytes + 255) / 256 * 256;
+constexpr size_t kScratchBytes = kOffWave + kWaveBytes;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+namespace {
+std::mutex g_mtx;
+void* g_addr[128] = {nullptr};
+bool g_const_ready[128] = {false};
+
+// Device address of the scratch array on the current device (looked up once per device).
+unsigned char* scratch_for_current_device(cudaStream_t st)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) throw MsError(MS_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    MS_REQUIRE(dev >= 0 && dev < 128, MS_ERR_NO_DEVICE, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_mtx);
+    if (!g_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            throw MsError(MS_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array: ") +
+                                           cudaGetErrorString(e));
+        g_addr[dev] = p;
+    }
+    if (!g_const_ready[dev]) {
+        upload_constants(st);
+        g_const_ready[dev] = true;
+    }
+    return (unsigned char*)g_addr[dev];
+}
+
+int team_size_of(int N)
+{
+    switch (N) {
+    case 128: return FftCfg<128>::G;
+    case 256: return FftCfg<256>::G;
+    case 512: return FftCfg<512>::G;
+    case 1024: return FftCfg<1024>::G;
+    case 2048: return FftCfg<2048>::G;
+    }
+    throw MsError(MS_ERR_UNSUPPORTED, "unsupported transform length");
+}
+
+void twiddle_table(int N, float2* out)
+{
+    const double pi = 3.14159265358979323846264338327950288;
+    int G = team_size_of(N), E = N / G;
+    for (int k1 = 0; k1 < E; k1++)
+        for (int g = 0; g < G; g++) {
+            double a = -2.0 * pi * (double)((int64_t)g * k1 % N) / (double)N;
+            out[(size_t)k1 * G + g] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+}
+
+void ck(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw MsError(MS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+}  // namespace
+
+size_t noalloc_scratch_bytes() { return kScratchBytes; }
+
+void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, int S, double z_init, const double* xy,
+                          int np, float* I)
+{
+    validate_params(p);
+    MS_REQUIRE(V && xy && I, MS_ERR_INVALID_ARG, "V, probe_xy and I must not be NULL");
+    MS_REQUIRE(S >= 1 && np >= 1, MS_ERR_INVALID_ARG, "need at least one slice and one probe");
+    MS_REQUIRE(p.n_det >= 1 && p.n_det <= MS_MAX_DET, MS_ERR_INVALID_ARG, "need 1..8 detectors");
+    const int64_t N = (int64_t)p.nx * p.ny;
+    MS_REQUIRE((size_t)N * sizeof(float2) <= kWaveBytes, MS_ERR_UNSUPPORTED,
+               "grid too large for the fixed scratch array: nx*ny*8 bytes must not exceed 32 MiB");
+    unsigned char* base = scratch_for_current_device(st);
+    float2* tw_x = (float2*)(base + kOffTables);
+    float2* tw_y = tw_x + kMaxN;
+    float2* prop_x = tw_y + kMaxN;
+    float2* prop_y = prop_x + kMaxN;
+    WaveInfo* dwv = (WaveInfo*)(base + kOffWaveInfo);
+    float* thr = (float*)(base + kOffThr);
+    double* Iw = (double*)(base + kOffIwave);
+    double* partial = (double*)(base + kOffPartial);
+    float2* psi = (float2*)(base + kOffWave);
+
+    Physics ph = physics_of(p.E0, p.theta);
+    GridConst gc = grid_of(p, ph);
+    std::vector<float2> tab(4 * (size_t)kMaxN);
+    twiddle_table(p.nx, tab.data());
+    twiddle_table(p.ny, tab.data() + kMaxN);
+    for (int i = 0; i < p.nx; i++) {
+        double g = (double)((i < p.nx / 2) ? i : i - p.nx) * gc.dgx - gc.g0x;
+        double th = gc.prop_w * g * g;
+        tab[2 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+    for (int i = 0; i < p.ny; i++) {
+        double g = (double)((i < p.ny / 2) ? i : i - p.ny) * gc.dgy - gc.g0y;
+        double th = gc.prop_w * g * g;
+        tab[3 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+    ck(cudaMemcpyAsync(tw_x, tab.data(), kTableBytes, cudaMemcpyHostToDevice, st), "table upload");
+    const int ndet = p.n_det;
+    float th_h[2 * MS_MAX_DET];
+    for (int d = 0; d < ndet; d++) {
+        th_h[d] = g2_threshold(p.det_inner[d], ph.lambda);
+        th_h[ndet + d] = g2_threshold(p.det_outer[d], ph.lambda);
+    }
+    ck(cudaMemcpyAsync(thr, th_h, sizeof(float) * 2 * ndet, cudaMemcpyHostToDevice, st), "threshold upload");
+
+    GridDev gd;
+    gd.nx = p.nx;
+    gd.ny = p.ny;
+    gd.dgx_f = gc.dgx_f;
+    gd.dgy_f = gc.dgy_f;
+    gd.dgx = gc.dgx;
+    gd.dgy = gc.dgy;
+    gd.gl2_f = (float)gc.gl2;
+    gd.alpha_f = (float)gc.alpha;
+    gd.bwl = p.bwl ? 1 : 0;
+    gd.inv_n = 1.0f / (float)N;
+    LensCoef lc = lens_coef(p.cond_lens, ph.lambda, 0.0);
+    LensDev lens;
+    std::memset(&lens, 0, sizeof(lens));
+    lens.m = lc.m; lens.phi_req = lc.phi_req;
+    lens.cc10 = lc.cc10; lens.cc12 = lc.cc12; lens.cc21 = lc.cc21; lens.cc23 = lc.cc23; lens.cc30 = lc.cc30;
+    lens.cc32 = lc.cc32; lens.cc34 = lc.cc34; lens.cc41 = lc.cc41; lens.cc43 = lc.cc43; lens.cc45 = lc.cc45;
+    lens.cc50 = lc.cc50; lens.cc52 = lc.cc52; lens.cc54 = lc.cc54; lens.cc56 = lc.cc56;
+    lens.p12 = lc.p12; lens.p21 = lc.p21; lens.p23 = lc.p23; lens.p32 = lc.p32; lens.p34 = lc.p34;
+    lens.p41 = lc.p41; lens.p43 = lc.p43; lens.p45 = lc.p45; lens.p52 = lc.p52; lens.p54 = lc.p54;
+    lens.p56 = lc.p56;
+    lens.g2min = lc.g2min;
+    lens.g2max = lc.g2max;
+
+    const int B = (int)std::min<int64_t>(std::min<int64_t>(kMaxBatch, np), (int64_t)(kWaveBytes / (N * 8)));
+    const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxBlk, N / 4096));
+    const double cc10 = gate_coef(-3.14159265358979323846 * (p.cond_lens.c10 + z_init) * ph.lambda);
+    std::vector<WaveInfo> wv((size_t)B);
+    for (int start = 0; start < np; start += B) {
+        const int nb = std::min(B, np - start);
+        for (int i = 0; i < nb; i++) {
+            wv[i].px = xy[2 * (start + i)];
+            wv[i].py = xy[2 * (start + i) + 1];
+            wv[i].cc10 = cc10;
+            wv[i].conf_slot = 0;
+            wv[i].n_slices = S;
+            wv[i].weight = 1.0f;
+            wv[i].pos = start + i;
+        }
+        ck(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nb, cudaMemcpyHostToDevice, st), "wave table upload");
+        PassArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.psi = psi;
+        a.waves = dwv;
+        a.sV = V;
+        a.sV_slot_stride = (int64_t)S * N;
+        a.prop_x = prop_x;
+        a.prop_y = prop_y;
+        a.grid = gd;
+        a.lens = lens;
+        a.tw = tw_y;
+        launch_col(p.ny, COL_PROBE_INV, a, nb, p.nx, st);
+        for (int sl = 0; sl < S; sl++) {
+            a.slice = sl;
+            a.tw = tw_x;
+            launch_row(p.nx, ROW_INV_T_FWD, a, nb, p.ny, st);
+            a.tw = tw_y;
+            launch_col(p.ny, COL_STEP, a, nb, p.nx, st);
+        }
+        launch_detect(psi, nb, p.nx, p.ny, gd.dgx_f, gd.dgy_f, thr, thr + ndet, ndet, partial, nblk, st);
+        launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw, nullptr, 0, 0, st);
+        launch_d2f(Iw, (int64_t)nb * ndet, I + (int64_t)start * ndet, st);
+        // the host wave table is rewritten for the next batch
+        ck(cudaStreamSynchronize(st), "stream synchronize");
+    }
+}
+
+}  // namespace msb

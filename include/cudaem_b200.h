@@ -234,6 +234,20 @@ ms_status ms_projected_potential(ms_ctx* ctx, const ms_params* p, const ms_atoms
 ms_status ms_stem_forward_potential(ms_ctx* ctx, const ms_params* p, const float* V, int n_slices,
                                     int V_on_device, double z_init, const double* probe_xy, int n_probe,
                                     float* I_out);
+/* The same computation as ms_stem_forward_potential for callers that cannot let a library
+ * allocate device memory (an application whose memory manager owns every allocation, or a
+ * loop that must not pay cudaMalloc's implicit synchronisation).  No reference counterpart:
+ * the reference allocates per call.  It allocates nothing and needs no context: V (device,
+ * [n_slices][ny][nx]) and I_out (device, [n_probe][n_det]) are the caller's device memory,
+ * probe_xy is host memory, and the work runs on `cuda_stream` (NULL = legacy default stream)
+ * of the current device.  All scratch -- waves, twiddles, propagator factors, detector
+ * partial sums -- lives in one fixed array of about 34 MiB held by every GPU that loads the
+ * library until exit; grids with nx*ny*8 bytes above 32 MiB (larger than 2048 x 2048) are
+ * rejected with MS_ERR_UNSUPPORTED.  The first call on each device looks the array up and
+ * should come before any stream capture.  All calls share the array, so calls that overlap
+ * on the GPU race and must be serialised.  Errors are read with ms_last_error(NULL). */
+ms_status ms_stem_forward_potential_noalloc(void* cuda_stream, const ms_params* p, const float* V, int n_slices,
+                                            double z_init, const double* probe_xy, int n_probe, float* I_out);
 /* Adjoint of ms_stem_forward_potential for the loss L = sum (I - target)^2:
  * loss, dL/dV [n_slices][ny][nx] (summed over probes) and dL/dC10, dL/dC30 of the condenser
  * lens.  Slices are checkpointed every p->ckpt_interval and recomputed.  No reference
