@@ -17,6 +17,8 @@ struct ms_ctx {
     double last_ms = 0.0;
     int64_t last_launches = 0;
     bool constants_ready = false;
+    std::string prop_key;                        // parameters of the cached propagator table
+    void* exptab = nullptr;                      // exp(2 pi i k / 1024), k < 1024
 
     struct Buf {
         void* p = nullptr;

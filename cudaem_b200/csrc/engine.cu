@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 
@@ -59,6 +60,9 @@ void ms_ctx::release_all()
     bufs.clear();
     for (auto& kv : twiddles) cudaFree(kv.second);
     twiddles.clear();
+    if (exptab) cudaFree(exptab);
+    exptab = nullptr;
+    prop_key.clear();
 }
 
 cudaEvent_t ms_ctx::prof_event()
@@ -141,15 +145,18 @@ const float2* twiddles(ms_ctx* c, int N)
     auto it = c->twiddles.find(N);
     if (it != c->twiddles.end()) return (const float2*)it->second;
     int G = team_size(N), E = N / G;
-    std::vector<float2> t((size_t)N);
+    std::vector<float2> t(2 * (size_t)N);  // high parts, then the rounded remainders
     for (int k1 = 0; k1 < E; k1++)
         for (int g = 0; g < G; g++) {
             double a = -2.0 * kPi * (double)((int64_t)g * k1 % N) / (double)N;
-            t[(size_t)k1 * G + g] = make_float2((float)std::cos(a), (float)std::sin(a));
+            double c = std::cos(a), s = std::sin(a);
+            float2 hi = make_float2((float)c, (float)s);
+            t[(size_t)k1 * G + g] = hi;
+            t[(size_t)N + k1 * G + g] = make_float2((float)(c - (double)hi.x), (float)(s - (double)hi.y));
         }
     void* p = nullptr;
-    CK(cudaMalloc(&p, sizeof(float2) * N));
-    CK(cudaMemcpy(p, t.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&p, sizeof(float2) * 2 * N));
+    CK(cudaMemcpy(p, t.data(), sizeof(float2) * 2 * N, cudaMemcpyHostToDevice));
     c->twiddles[N] = p;
     return (const float2*)p;
 }
@@ -178,6 +185,8 @@ struct Setup {
     const float2* tw_y;
     const float2* prop_x;
     const float2* prop_y;
+    const float2* prop;
+    const float2* exptab;
     int64_t N;
 };
 
@@ -217,6 +226,27 @@ Setup make_setup(ms_ctx* c, const ms_params& p)
     CK(cudaMemcpyAsync(dpy, py.data(), sizeof(float2) * p.ny, cudaMemcpyHostToDevice, c->stream));
     s.prop_x = dpx;
     s.prop_y = dpy;
+    // full table P(k), rebuilt only when the grid, wavelength, slice thickness or tilt change
+    char key[256];
+    std::snprintf(key, sizeof(key), "%d,%d,%.17g,%.17g,%.17g,%.17g,%.17g,%d", p.nx, p.ny, p.lx, p.ly, s.gc.prop_w,
+                  s.gc.g0x, s.gc.g0y, p.bwl);
+    float2* P = (float2*)c->buf("prop", sizeof(float2) * s.N);
+    if (c->prop_key != key) {
+        launch_prop_table(p.nx, p.ny, s.gc.dgx, s.gc.dgy, s.gc.g0x, s.gc.g0y, s.gc.prop_w, s.gc.alpha, s.gc.gl2,
+                          p.bwl ? 1 : 0, P, c->stream);
+        c->prop_key = key;
+    }
+    s.prop = P;
+    if (!c->exptab) {
+        std::vector<float2> e(1024);
+        for (int k = 0; k < 1024; k++) {
+            double a = 2.0 * kPi * k / 1024.0;
+            e[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        CK(cudaMalloc(&c->exptab, sizeof(float2) * 1024));
+        CK(cudaMemcpy(c->exptab, e.data(), sizeof(float2) * 1024, cudaMemcpyHostToDevice));
+    }
+    s.exptab = (const float2*)c->exptab;
     return s;
 }
 
@@ -402,6 +432,10 @@ PotArgs pot_args(const ms_params& p, const Setup& s, const AtomsDev& A, const Sp
     a.dy = (float)s.gc.dy;
     a.lx = (float)p.lx;
     a.ly = (float)p.ly;
+    a.dx_hi = (float)s.gc.dx;
+    a.dx_lo = (float)(s.gc.dx - (double)a.dx_hi);
+    a.dy_hi = (float)s.gc.dy;
+    a.dy_lo = (float)(s.gc.dy - (double)a.dy_hi);
     a.wrap = p.pot_wrap ? 1 : 0;
     a.elems = A.tables;
     a.n_elem = A.n_elem;
@@ -420,6 +454,8 @@ PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const flo
     a.sV_slice_base = 0;
     a.prop_x = s.prop_x;
     a.prop_y = s.prop_y;
+    a.prop = s.prop;
+    a.exptab = s.exptab;
     a.grid = s.gd;
     a.lens = lens;
     return a;

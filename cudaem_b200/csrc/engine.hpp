@@ -54,9 +54,12 @@ float g2_threshold(double angle, double lambda);
 
 // Radial spline of one element in the device layout (VR_Cubic coefficients of
 // Element_Coeffs_Dev, device_containers.cuh:243-249).
+struct ElemCoef4 {
+    float c0, c1, c2, c3;
+};
 struct ElemTable {
     float R2[MS_NR];
-    float c0[MS_NR], c1[MS_NR], c2[MS_NR], c3[MS_NR];
+    ElemCoef4 c[MS_NR];   // cubic coefficients of node i, packed for one 16-byte load
     float rmax, rmax2;
     float l0, inv_dl;   // log2(R2[0]) and nodes per log2 unit, for the direct index guess
     int Z;

@@ -40,14 +40,16 @@ struct FftLayout {
     static constexpr int TC = FftCfg<N>::TC;
     static constexpr int ROW_THREADS = ROWS * G;
     static constexpr int COL_THREADS = TC * G;
+    static constexpr int COL_MINB = (N == 2048) ? 1 : 2;   // resident column blocks per SM (register cap)
     // transpose scratch of one transform: E rows of G+1 slots, plus padding so that
     // consecutive transforms start on banks that keep a half-warp conflict-free
     static constexpr int SCR_BASE = E * (G + 1);
     static constexpr int SCR_STRIDE_ROW = SCR_BASE + 1;
     static constexpr int SCR_STRIDE_COL =
         (TC == 16) ? (SCR_BASE + ((1 - SCR_BASE % 16) + 16) % 16) : (SCR_BASE + ((2 - SCR_BASE % 16) + 16) % 16);
-    static constexpr size_t ROW_SMEM = sizeof(float2) * ((size_t)ROWS * SCR_STRIDE_ROW + N);
-    static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + N);
+    // transpose scratch, twiddles (high and low parts), and the 1024-entry exp(i phi) table
+    static constexpr size_t ROW_SMEM = sizeof(float2) * ((size_t)ROWS * SCR_STRIDE_ROW + 2 * N + 1024);
+    static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + 2 * N);
 };
 
 }  // namespace msb

@@ -252,15 +252,15 @@ void build_elem_table(const ms_params& p, int Z, ElemTable* t)
     std::memset(t, 0, sizeof(*t));
     for (int i = 0; i < MS_NR; i++) {
         t->R2[i] = (float)R2[i];
-        t->c0[i] = (float)c0[i];
-        t->c1[i] = (float)c1[i];
+        t->c[i].c0 = (float)c0[i];
+        t->c[i].c1 = (float)c1[i];
     }
     for (int i = 0; i < MS_NR - 1; i++) {  // get_cubic_poly_coef (basic_functions_dev.cuh:76-89)
         double idR = 1.0 / (R2[i + 1] - R2[i]);
         double m = (c0[i + 1] - c0[i]) * idR;
         double n = c1[i] + c1[i + 1];
-        t->c2[i] = (float)((3.0 * m - n - c1[i]) * idR);
-        t->c3[i] = (float)((n - 2.0 * m) * idR * idR);
+        t->c[i].c2 = (float)((3.0 * m - n - c1[i]) * idR);
+        t->c[i].c3 = (float)((n - 2.0 * m) * idR * idR);
     }
     t->rmax = (float)rmx;
     t->rmax2 = (float)(rmx * rmx);

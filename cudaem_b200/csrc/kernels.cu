@@ -32,12 +32,15 @@ static void check_launch(const char* what)
 
 void upload_constants(cudaStream_t st)
 {
-    float2 t[64];
+    float2 t[64], tl[64];
     for (int m = 0; m < 64; m++) {
         double a = -2.0 * 3.14159265358979323846264338327950288 * m / 64.0;
-        t[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+        double c = std::cos(a), sn = std::sin(a);
+        t[m] = make_float2((float)c, (float)sn);
+        tl[m] = make_float2((float)(c - (double)t[m].x), (float)(sn - (double)t[m].y));
     }
     cudaError_t e = cudaMemcpyToSymbolAsync(c_tw64, t, sizeof(t), 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(c_tw64_lo, tl, sizeof(tl), 0, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) throw MsError(MS_ERR_CUDA, std::string("constant upload: ") + cudaGetErrorString(e));
 }
 
@@ -73,6 +76,38 @@ __device__ __forceinline__ float2 expi_d(double ph)
 
 __device__ __forceinline__ double freq_d(int i, int n, double dg) { return (double)((i < n / 2) ? i : i - n) * dg; }
 
+// exp(i phi) for the transmission: phi = k h + d with h = 2 pi / 1024 (Cody-Waite split, exact
+// product for |k| < 4096), exp(i k h) from a table rounded from FP64, and exp(i d) for
+// |d| <= pi/1024 from its Taylor series to d^4 / d^5 (truncation below 3e-15).  The result
+// carries about one ulp of error, like sincosf, at a third of its instructions.
+constexpr int kExpTab = 1024;
+__device__ __forceinline__ float2 expi_tab(float phi, const float2* __restrict__ tab)
+{
+    const float kf = rintf(phi * 162.97466172610083f);
+    float d = fmaf(-kf, 0.006134033203125f, phi);
+    d = fmaf(-kf, 1.8899484075518558e-06f, d);
+    const float2 T = tab[(int)kf & (kExpTab - 1)];
+    const float d2 = d * d;
+    const float c = fmaf(d2, fmaf(d2, 0.041666666666666664f, -0.5f), 1.0f);
+    const float s = d * fmaf(d2, -0.16666666666666666f, 1.0f);
+    return make_float2(T.x * c - T.y * s, T.x * s + T.y * c);
+}
+
+// Hides a pointer's provenance from the optimiser (no instruction is emitted).
+template <class T>
+__device__ __forceinline__ T* opaque(T* p)
+{
+    asm volatile("" : "+l"(p));
+    return p;
+}
+
+template <int E>
+__device__ __forceinline__ void conj_all(float2 (&v)[E])
+{
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j].y = -v[j].y;
+}
+
 // ---------------------------------------------------------------------------
 // row pass
 // ---------------------------------------------------------------------------
@@ -92,7 +127,10 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
     if ((OP == ROW_T_FWD || OP == ROW_INV_T_FWD) && beyond && !(a.flags & PF_VACUUM_BEYOND)) return;
 
     float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = a.tw[i];
+    float2* etab = tw + 2 * N;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD)
+        for (int i = threadIdx.x; i < kExpTab; i += blockDim.x) etab[i] = a.exptab[i];
     __syncthreads();
     float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
     auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
@@ -100,29 +138,38 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
 
     const size_t row_off = ((size_t)b * ny + r) * N;
     float2 v[E];
-    if (OP == ROW_T_FWD) {
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD) {
+        const float* vr =
+            a.sV + (size_t)wi.conf_slot * a.sV_slot_stride + ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
+        if (OP == ROW_T_FWD) {
 #pragma unroll
-        for (int j = 0; j < E; j++) v[j] = make_float2(1.0f, 0.0f);
+            for (int j = 0; j < E; j++) v[j] = make_float2(1.0f, 0.0f);
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = a.psi[row_off + g + G * j];
+        }
+        // pass 0: inverse row FFT as conj(FFT(conj(x))), then the transmission;
+        // pass 1: forward row FFT.  One copy of the transform code serves both.
+#pragma unroll 1
+        for (int pass = (OP == ROW_T_FWD) ? 1 : 0; pass < 2; pass++) {
+            if (pass == 0) conj_all(v);
+            else if (!beyond) {
+#pragma unroll
+                for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + g + G * j), etab));
+            }
+            team_fft<N, G, -1>(v, g, tw, scr, sync);
+            if (pass == 0) conj_all(v);
+        }
+#pragma unroll
+        for (int j = 0; j < E; j++) a.psi[row_off + g + G * j] = v[j];
+        return;
     } else {
         const float2* src = (OP == ROW_INV_ABS2 && (a.flags & PF_FILTER_AUX)) ? a.aux : a.psi;
 #pragma unroll
         for (int j = 0; j < E; j++) v[j] = src[row_off + g + G * j];
         team_fft<N, G, +1>(v, g, tw, scr, sync);
     }
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD) {
-        if (!beyond) {
-            const float* vr = a.sV + (size_t)wi.conf_slot * a.sV_slot_stride + ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
-#pragma unroll
-            for (int j = 0; j < E; j++) {
-                float s, c;
-                sincosf(__ldg(vr + g + G * j), &s, &c);
-                v[j] = cmul(v[j], make_float2(c, s));
-            }
-        }
-        team_fft<N, G, -1>(v, g, tw, scr, sync);
-#pragma unroll
-        for (int j = 0; j < E; j++) a.psi[row_off + g + G * j] = v[j];
-    } else if (OP == ROW_INV_ABS2) {
+    if (OP == ROW_INV_ABS2) {
         float* o = a.out_real + ((a.flags & PF_FILTER_AUX) ? (size_t)r * N : row_off);
         const float w = wi.weight;
 #pragma unroll
@@ -141,7 +188,7 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
 // column pass
 // ---------------------------------------------------------------------------
 template <int N, int OP>
-__global__ void __launch_bounds__(FftLayout<N>::COL_THREADS) k_col(PassArgs a)
+__global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_MINB) k_col(PassArgs a)
 {
     using L = FftLayout<N>;
     constexpr int G = L::G, E = L::E, TC = L::TC;
@@ -154,19 +201,24 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS) k_col(PassArgs a)
     const int col = col0 + c;
     const WaveInfo wi = a.waves[b];
     bool final_step = false;
-    if (OP == COL_STEP) {
+    if (OP == COL_STEP || OP == COL_STEP_SEP) {
         if (a.slice >= wi.n_slices && !(a.flags & PF_VACUUM_BEYOND)) return;
         final_step = (a.slice == wi.n_slices - 1) && !(a.flags & PF_PROP_ALWAYS);
     }
 
     float2* tw = smem + TC * L::SCR_STRIDE_COL;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = a.tw[i];
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
     __syncthreads();
     float2* scr_base = smem + c * L::SCR_STRIDE_COL;
     auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
     auto sync = []() { __syncthreads(); };
 
     float2* base = a.psi + (size_t)b * N * nx;
+    // element (g + G j, col) of the wave sits at cp[j * cs]; the pointer is made opaque before each
+    // later use so the compiler recomputes the E addresses (one IMAD each) instead of keeping E
+    // 64-bit addresses live across the transforms
+    float2* cp = base + (size_t)g * nx + col;
+    const size_t cs = (size_t)G * nx;
     float2 v[E];
     if constexpr (OP == COL_PROBE_INV) {
         // Generate_probe / Generate_multi_probe (device_kernels.cuh:363-444): aperture mask on the
@@ -185,38 +237,58 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS) k_col(PassArgs a)
             }
         }
         team_fft<N, G, +1>(v, g, tw, scr, sync);
+        cp = opaque(cp);
 #pragma unroll
-        for (int j = 0; j < E; j++) base[(size_t)(g + G * j) * nx + col] = v[j];
+        for (int j = 0; j < E; j++) cp[j * cs] = v[j];
         return;
     } else {
 #pragma unroll
-    for (int j = 0; j < E; j++) v[j] = base[(size_t)(g + G * j) * nx + col];
+    for (int j = 0; j < E; j++) v[j] = cp[j * cs];
 
-    if (OP == COL_STEP) {
-        team_fft<N, G, -1>(v, g, tw, scr, sync);
-        if (final_step) {
-#pragma unroll
-            for (int j = 0; j < E; j++) base[(size_t)(g + G * j) * nx + col] = v[j];
-            return;
-        }
-        // P(k) = (1/N) bwl(g^2) exp(i w |g - g0|^2), separable phase (gen_propagator_kernel,
-        // device_kernels.cuh:215-234)
-        const float2 px = __ldg(a.prop_x + col);
-#pragma unroll
-        for (int j = 0; j < E; j++) {
-            const int k = g + G * j;
-            float amp = a.grid.inv_n;
-            float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
-            if (a.grid.bwl) amp = amp / (1.0f + expf(a.grid.alpha_f * (g2 - a.grid.gl2_f)));
-            float2 pr = cmul(px, __ldg(a.prop_y + k));
-            v[j] = cmul(v[j], cscale(pr, amp));
-            if (a.flags & PF_FILTER_AUX) {
-                float2* ab = a.aux + (size_t)b * N * nx;
-                bool in = (a.filt_g2in <= g2 && g2 <= a.filt_g2out);
-                ab[(size_t)k * nx + col] = in ? v[j] : make_float2(0.0f, 0.0f);
+    if (OP == COL_STEP || OP == COL_STEP_SEP) {
+        // pass 0: forward column FFT, then P (or stop: the exit wave of the wave's last slice);
+        // pass 1: inverse column FFT as conj(FFT(conj(x))).  One copy of the transform code.
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {
+            team_fft<N, G, -1>(v, g, tw, scr, sync);
+            if (pass == 1) {
+                conj_all(v);
+                break;
             }
+            if (final_step) break;
+            if (OP == COL_STEP) {
+                // P(k) = (1/N) bwl(g^2) exp(i w |g - g0|^2) (gen_propagator_kernel, device_kernels.cuh:215-234),
+                // tabulated once per grid in FP64 and rounded to FP32; shared by every wave, so it stays in L2.
+                // The barrier keeps the table loads after the transform, so they do not hold registers
+                // across it.
+                const float2* pp = opaque(a.prop + (size_t)g * nx + col);
+#pragma unroll
+                for (int j = 0; j < E; j++) v[j] = cmul(v[j], __ldg(pp + j * cs));
+            } else {
+                // P formed per element from the separable FP64-rounded phase factors and the band limit
+                // (where no table may be stored)
+                const float2 px = __ldg(a.prop_x + col);
+#pragma unroll
+                for (int j = 0; j < E; j++) {
+                    const int k = g + G * j;
+                    float amp = a.grid.inv_n;
+                    float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+                    if (a.grid.bwl) amp = amp / (1.0f + expf(a.grid.alpha_f * (g2 - a.grid.gl2_f)));
+                    v[j] = cmul(v[j], cscale(cmul(px, __ldg(a.prop_y + k)), amp));
+                }
+            }
+            if (a.flags & PF_FILTER_AUX) {
+                float2* ab = opaque(a.aux + (size_t)b * N * nx + (size_t)g * nx + col);
+#pragma unroll
+                for (int j = 0; j < E; j++) {
+                    const int k = g + G * j;
+                    float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+                    bool in = (a.filt_g2in <= g2 && g2 <= a.filt_g2out);
+                    ab[j * cs] = in ? v[j] : make_float2(0.0f, 0.0f);
+                }
+            }
+            conj_all(v);
         }
-        team_fft<N, G, +1>(v, g, tw, scr, sync);
     } else if (OP == COL_CTF_INV) {
         // apply_CTF_kernel (device_kernels.cuh:445-468)
         const double gx = freq_d(col, nx, a.grid.dgx);
@@ -235,8 +307,9 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS) k_col(PassArgs a)
     } else if (OP == COL_INV) {
         team_fft<N, G, +1>(v, g, tw, scr, sync);
     }
+    cp = opaque(cp);
 #pragma unroll
-    for (int j = 0; j < E; j++) base[(size_t)(g + G * j) * nx + col] = v[j];
+    for (int j = 0; j < E; j++) cp[j * cs] = v[j];
     }
 }
 
@@ -289,7 +362,35 @@ static void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStre
         cudaFuncSetAttribute(k_col<N, COL_CTF_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_col<N, COL_CTF_INV><<<grid, block, sm, st>>>(a);
         break;
+    case COL_STEP_SEP:
+        cudaFuncSetAttribute(k_col<N, COL_STEP_SEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_STEP_SEP><<<grid, block, sm, st>>>(a);
+        break;
     }
+}
+
+// Full propagator table in FP64, rounded to FP32 (gen_propagator_kernel, device_kernels.cuh:215-234)
+__global__ void k_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
+                             double gl2, int bwl, double inv_n, float2* P)
+{
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y;
+    if (ix >= nx) return;
+    double gx = freq_d(ix, nx, dgx), gy = freq_d(iy, ny, dgy);
+    double amp = inv_n;
+    if (bwl) amp = amp / (1.0 + exp(alpha * (gx * gx + gy * gy - gl2)));
+    double th = w * ((gx - g0x) * (gx - g0x) + (gy - g0y) * (gy - g0y));
+    double s, c;
+    sincos(th, &s, &c);
+    P[(size_t)iy * nx + ix] = make_float2((float)(amp * c), (float)(amp * s));
+}
+
+void launch_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
+                       double gl2, int bwl, float2* P, cudaStream_t st)
+{
+    k_prop_table<<<dim3((nx + 127) / 128, ny), 128, 0, st>>>(nx, ny, dgx, dgy, g0x, g0y, w, alpha, gl2, bwl,
+                                                             1.0 / ((double)nx * ny), P);
+    count_launch();
+    check_launch("propagator table");
 }
 
 void launch_row(int N, int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st)
@@ -349,7 +450,8 @@ size_t col_smem(int N)
 // projected potential: gen_slice_potential_kernel (device_kernels.cuh:28-47)
 // restructured as atom-culled 64x16 pixel tiles with float4 stores
 // ---------------------------------------------------------------------------
-constexpr int kPotTX = 64, kPotTY = 16, kPotThreads = 256, kPotMaxImg = 4;
+constexpr int kPotTX = 64, kPotTY = 32, kPotThreads = 256, kPotMaxImg = 4;
+constexpr int kPotRowsPerThread = kPotTY / (kPotThreads / (kPotTX / 4));   // 2 rows of 4 pixels
 
 __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
 {
@@ -361,8 +463,23 @@ __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
     if (r2 < T.R2[i]) i = max(i - 1, 0);
     else if (i < MS_NR - 2 && r2 >= T.R2[i + 1]) i = i + 1;
     float d = r2 - T.R2[i];
-    return ((T.c3[i] * d + T.c2[i]) * d + T.c1[i]) * d + T.c0[i];  // get_value_Cubic_Spline
+    const ElemCoef4 c = T.c[i];
+    return ((c.c3 * d + c.c2) * d + c.c1) * d + c.c0;  // get_value_Cubic_Spline
 }
+
+// Up to four periodic images of an atom kept in registers (no indexed local array).
+struct ImgList {
+    float4 v0, v1, v2, v3;
+    int n = 0;
+    __device__ __forceinline__ void push(float4 v)
+    {
+        if (n == 0) v0 = v;
+        else if (n == 1) v1 = v;
+        else if (n == 2) v2 = v;
+        else if (n == 3) v3 = v;
+        n = min(n + 1, kPotMaxImg);
+    }
+};
 
 __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
 {
@@ -376,8 +493,17 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
     const int sl = a.slice0 + blockIdx.y;
     const int tiles_x = a.nx / kPotTX;
     const int tx0 = (blockIdx.x % tiles_x) * kPotTX, ty0 = (blockIdx.x / tiles_x) * kPotTY;
-    const int t = threadIdx.x, px = t % (kPotTX / 4), py = t / (kPotTX / 4);
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    // Each warp owns a compact 16x16-pixel block of the 64x32 tile (4 x 2 blocks), each lane 4 pixels
+    // in x on 2 rows, so a candidate atom far from a warp's block is skipped by the whole warp.
+    const int t = threadIdx.x, wblk = t >> 5, ln = t & 31;
+    const int px = (wblk % 4) * 4 + (ln % 4);          // in units of 4 pixels across the tile
+    const int py = (wblk / 4) * 16 + (ln / 4);         // first row of the lane inside the tile
+    constexpr int RY = kPotRowsPerThread, ROW_STEP = 8;
+    float acc[RY][4];
+#pragma unroll
+    for (int r = 0; r < RY; r++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) acc[r][k] = 0.f;
 
     if (sl < a.ns[conf]) {
         {
@@ -391,29 +517,28 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
         const int64_t s1 = a.seg[(int64_t)conf * (a.S_cap + 1) + sl + 1];
         const float X0 = (float)tx0 * a.dx, X1 = (float)(tx0 + kPotTX - 1) * a.dx;
         const float Y0 = (float)ty0 * a.dy, Y1 = (float)(ty0 + kPotTY - 1) * a.dy;
-        const float Y = (float)(ty0 + py) * a.dy;
-        float X[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) X[k] = (float)(tx0 + 4 * px + k) * a.dx;
         const int lane = t & 31, wid = t >> 5;
         for (int64_t base = s0; base < s1; base += kPotThreads) {
             int64_t i = base + t;
-            float4 cimg[kPotMaxImg];
-            int cnt = 0;
+            ImgList im;
             if (i < s1) {
-                float xa = a.ax[i], ya = a.ay[i], w = a.aw[i];
-                int e = a.ae[i];
-                float rm = el[e].rmax * 1.0001f + 1e-4f;
-                const int lo = a.wrap ? -1 : 0, hi = a.wrap ? 1 : 0;
-                for (int iy = lo; iy <= hi; iy++)
-                    for (int ix = lo; ix <= hi; ix++) {
-                        float xs = xa + ix * a.lx, ys = ya + iy * a.ly;
+                const float xa = a.ax[i], ya = a.ay[i], w = a.aw[i];
+                const int e = a.ae[i];
+                const float rm = el[e].rmax * 1.0001f + 1e-4f;
+#pragma unroll
+                for (int iy = -1; iy <= 1; iy++)
+#pragma unroll
+                    for (int ix = -1; ix <= 1; ix++) {
+                        if (!a.wrap && (ix != 0 || iy != 0)) continue;
+                        // culling only: approximate image position
+                        float xs = xa + (float)ix * a.lx, ys = ya + (float)iy * a.ly;
                         float dxr = fmaxf(0.f, fmaxf(X0 - xs, xs - X1));
                         float dyr = fmaxf(0.f, fmaxf(Y0 - ys, ys - Y1));
-                        if (dxr * dxr + dyr * dyr < rm * rm && cnt < kPotMaxImg)
-                            cimg[cnt++] = make_float4(xs, ys, w, __int_as_float(e));
+                        if (dxr * dxr + dyr * dyr < rm * rm)
+                            im.push(make_float4(xa, ya, w, __int_as_float(e | ((ix + 1) << 8) | ((iy + 1) << 10))));
                     }
             }
+            const int cnt = im.n;
             // ordered compaction (deterministic: atom order, then image order)
             int incl = cnt;
 #pragma unroll
@@ -433,29 +558,53 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
                 total_s = run;
             }
             __syncthreads();
-            int off = wsum[wid] + incl - cnt;
-            for (int q = 0; q < cnt; q++) cand[off + q] = cimg[q];
+            const int off = wsum[wid] + incl - cnt;
+            if (cnt > 0) cand[off] = im.v0;
+            if (cnt > 1) cand[off + 1] = im.v1;
+            if (cnt > 2) cand[off + 2] = im.v2;
+            if (cnt > 3) cand[off + 3] = im.v3;
             __syncthreads();
             const int total = total_s;
             for (int q = 0; q < total; q++) {
-                float4 cd = cand[q];
-                const ElemTable& T = el[__float_as_int(cd.w)];
-                float dy = Y - cd.y;
-                float dy2 = dy * dy;
+                const float4 cd = cand[q];
+                const int bits = __float_as_int(cd.w);
+                const ElemTable& T = el[bits & 0xFF];
+                const float rmax2 = T.rmax2;
+                // distance to the image (ox, oy) of the atom: pixel index shifted by -ox*nx, and
+                // i*dx - x formed with dx split in two floats, so the offset is accurate to its own
+                // rounding (the pixel coordinate i*dx alone would carry ~1e-6 A of error)
+                const int ox = ((bits >> 8) & 3) - 1, oy = ((bits >> 10) & 3) - 1;
+                const float fx0 = (float)(tx0 + 4 * px - ox * a.nx), fy0 = (float)(ty0 + py - oy * a.ny);
+                float dx2[4], dy2[RY];
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
-                    float dx = X[k] - cd.x;
-                    float r2 = dx * dx + dy2;
-                    if (r2 < T.rmax2) acc[k] += cd.z * spline_eval(T, r2);
+                    const float fx = fx0 + (float)k;
+                    const float d = fmaf(fx, a.dx_lo, fmaf(fx, a.dx_hi, -cd.x));
+                    dx2[k] = d * d;
+                }
+#pragma unroll
+                for (int r = 0; r < RY; r++) {
+                    const float fy = fy0 + (float)(r * ROW_STEP);
+                    const float d = fmaf(fy, a.dy_lo, fmaf(fy, a.dy_hi, -cd.y));
+                    dy2[r] = d * d;
+                }
+#pragma unroll
+                for (int r = 0; r < RY; r++) {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const float r2 = dx2[k] + dy2[r];
+                        if (r2 < rmax2) acc[r][k] += cd.z * spline_eval(T, r2);
+                    }
                 }
             }
             __syncthreads();
         }
     }
-    if (sl < a.slice0 + a.nslice) {
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
         float* out = a.V + (int64_t)conf * a.V_conf_stride + (int64_t)(sl - a.V_slice_base) * a.nx * a.ny +
-                     (int64_t)(ty0 + py) * a.nx + tx0 + 4 * px;
-        *reinterpret_cast<float4*>(out) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+                     (int64_t)(ty0 + py + r * ROW_STEP) * a.nx + tx0 + 4 * px;
+        *reinterpret_cast<float4*>(out) = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
     }
 }
 

@@ -34,7 +34,7 @@ struct LensDev {
 };
 
 enum RowOp { ROW_T_FWD = 0, ROW_INV_T_FWD = 1, ROW_INV_ABS2 = 2, ROW_INV_STORE = 3 };
-enum ColOp { COL_PROBE_INV = 0, COL_STEP = 1, COL_INV = 2, COL_CTF_INV = 3 };
+enum ColOp { COL_PROBE_INV = 0, COL_STEP = 1, COL_INV = 2, COL_CTF_INV = 3, COL_STEP_SEP = 4 };
 
 enum PassFlags {
     PF_VACUUM_BEYOND = 1,  // slices past a wave's own count are empty (t = 1) instead of skipped
@@ -56,6 +56,8 @@ struct PassArgs {
     const float2* tw;         // inter-level twiddles for this pass's length
     const float2* prop_x;     // [nx] exp(i w (gx - g0x)^2)
     const float2* prop_y;     // [ny] exp(i w (gy - g0y)^2)
+    const float2* prop;       // [ny][nx] full propagator P(k) including 1/N and the band limit
+    const float2* exptab;     // [1024] exp(2 pi i k / 1024) for the transmission
     GridDev grid;
     LensDev lens;
     float filt_g2in, filt_g2out;
@@ -76,6 +78,7 @@ struct PotArgs {
     int V_slice_base;           // slice index stored at V's slice 0
     int nx, ny;
     float dx, dy, lx, ly;
+    float dx_hi, dx_lo, dy_hi, dy_lo;  // sampling split in two floats: ix*dx - x is formed to float accuracy
     int wrap;
     const ElemTable* elems;
     int n_elem;
@@ -88,6 +91,8 @@ void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream
 size_t row_smem(int N);
 size_t col_smem(int N);
 void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st);
+void launch_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
+                       double gl2, int bwl, float2* P, cudaStream_t st);
 
 // specimen on the device
 void launch_displace(const float* x, const float* y, const float* z, const float* sig, int64_t n, const int* confs,

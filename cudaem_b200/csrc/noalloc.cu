@@ -37,7 +37,9 @@ constexpr size_t kWaveBytes = size_t(32) << 20;       // probe-batch waves: nx*n
 constexpr int kMaxBatch = 256;
 constexpr int kMaxN = 2048;
 constexpr int kMaxBlk = 64;
-constexpr size_t kTableBytes = sizeof(float2) * 4 * kMaxN;                             // tw_x, tw_y, prop_x, prop_y
+constexpr int kExpN = 1024;
+// tw_x and tw_y (high then low parts, 2 kMaxN each), prop_x, prop_y, exp table
+constexpr size_t kTableBytes = sizeof(float2) * (6 * kMaxN + kExpN);
 constexpr size_t kWaveInfoBytes = sizeof(WaveInfo) * kMaxBatch;
 constexpr size_t kThrBytes = 256;                                                     // 2 * MS_MAX_DET floats
 constexpr size_t kIwaveBytes = sizeof(double) * kMaxBatch * MS_MAX_DET;
@@ -95,12 +97,16 @@ int team_size_of(int N)
 
 void twiddle_table(int N, float2* out)
 {
+    // high parts at out[0, N), rounded remainders at out[N, 2N)
     const double pi = 3.14159265358979323846264338327950288;
     int G = team_size_of(N), E = N / G;
     for (int k1 = 0; k1 < E; k1++)
         for (int g = 0; g < G; g++) {
             double a = -2.0 * pi * (double)((int64_t)g * k1 % N) / (double)N;
-            out[(size_t)k1 * G + g] = make_float2((float)std::cos(a), (float)std::sin(a));
+            double c = std::cos(a), s = std::sin(a);
+            float2 hi = make_float2((float)c, (float)s);
+            out[(size_t)k1 * G + g] = hi;
+            out[(size_t)N + k1 * G + g] = make_float2((float)(c - (double)hi.x), (float)(s - (double)hi.y));
         }
 }
 
@@ -124,9 +130,10 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
                "grid too large for the fixed scratch array: nx*ny*8 bytes must not exceed 32 MiB");
     unsigned char* base = scratch_for_current_device(st);
     float2* tw_x = (float2*)(base + kOffTables);
-    float2* tw_y = tw_x + kMaxN;
-    float2* prop_x = tw_y + kMaxN;
+    float2* tw_y = tw_x + 2 * kMaxN;
+    float2* prop_x = tw_y + 2 * kMaxN;
     float2* prop_y = prop_x + kMaxN;
+    float2* exptab = prop_y + kMaxN;
     WaveInfo* dwv = (WaveInfo*)(base + kOffWaveInfo);
     float* thr = (float*)(base + kOffThr);
     double* Iw = (double*)(base + kOffIwave);
@@ -135,18 +142,22 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
 
     Physics ph = physics_of(p.E0, p.theta);
     GridConst gc = grid_of(p, ph);
-    std::vector<float2> tab(4 * (size_t)kMaxN);
+    std::vector<float2> tab(6 * (size_t)kMaxN + kExpN);
+    for (int k = 0; k < kExpN; k++) {
+        double e = 2.0 * 3.14159265358979323846264338327950288 * k / (double)kExpN;
+        tab[6 * (size_t)kMaxN + k] = make_float2((float)std::cos(e), (float)std::sin(e));
+    }
     twiddle_table(p.nx, tab.data());
-    twiddle_table(p.ny, tab.data() + kMaxN);
+    twiddle_table(p.ny, tab.data() + 2 * kMaxN);
     for (int i = 0; i < p.nx; i++) {
         double g = (double)((i < p.nx / 2) ? i : i - p.nx) * gc.dgx - gc.g0x;
         double th = gc.prop_w * g * g;
-        tab[2 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
+        tab[4 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
     }
     for (int i = 0; i < p.ny; i++) {
         double g = (double)((i < p.ny / 2) ? i : i - p.ny) * gc.dgy - gc.g0y;
         double th = gc.prop_w * g * g;
-        tab[3 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
+        tab[5 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
     }
     ck(cudaMemcpyAsync(tw_x, tab.data(), kTableBytes, cudaMemcpyHostToDevice, st), "table upload");
     const int ndet = p.n_det;
@@ -205,6 +216,7 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
         a.sV_slot_stride = (int64_t)S * N;
         a.prop_x = prop_x;
         a.prop_y = prop_y;
+        a.exptab = exptab;
         a.grid = gd;
         a.lens = lens;
         a.tw = tw_y;
@@ -214,7 +226,7 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
             a.tw = tw_x;
             launch_row(p.nx, ROW_INV_T_FWD, a, nb, p.ny, st);
             a.tw = tw_y;
-            launch_col(p.ny, COL_STEP, a, nb, p.nx, st);
+            launch_col(p.ny, COL_STEP_SEP, a, nb, p.nx, st);
         }
         launch_detect(psi, nb, p.nx, p.ny, gd.dgx_f, gd.dgy_f, thr, thr + ndet, ndet, partial, nblk, st);
         launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw, nullptr, 0, 0, st);

@@ -106,6 +106,35 @@ def test_stem_batch_sizes_agree(ctx):
     assert rel_l2(res[1], res[0]) < 1e-6 and rel_l2(res[2], res[0]) < 1e-6
 
 
+def test_full_size_cbed_one_configuration(ctx):
+    """The measured CBED workload at its real depth and sampling (Si 16x16x60 cells, 1024^2,
+    240 slices) for one phonon configuration: FP32 error after 240 slices stays within 1e-5."""
+    from cudaem_b200 import workloads as wl
+    p, at = wl.cbed_si(nconf=1)
+    out = cb.MulSimulator(ctx=ctx).executionCBED(p, at)
+    assert out.n_slices == 240
+    ref = orc.simulate_cbed(p, at)
+    assert rel_l2(out.image_intensity, ref) < TOL
+
+
+def test_full_size_hrtem(ctx):
+    """The measured HRTEM workload (SrTiO3 10x10x20 cells, 512^2, 40 slices, -10 nm, Cs 1 mm)."""
+    from cudaem_b200 import workloads as wl
+    p, at = wl.hrtem_sto()
+    out = cb.MulSimulator(ctx=ctx).executionTEM(p, at)
+    ref = orc.simulate_tem(p, at)
+    assert rel_l2(out.image_intensity, ref) < TOL
+
+
+def test_full_size_stem_probes(ctx):
+    """Two probes of the measured STEM workload (SrTiO3 16x16x25, 1024^2, 50 slices, ADF 60-200 mrad)."""
+    from cudaem_b200 import workloads as wl
+    p, at = wl.stem_sto(nconf=1, scan=(2, 1), step=0.8)
+    out = cb.MulSimulator(ctx=ctx).executionSTEM(p, at)
+    ref = orc.simulate_stem(p, at)
+    assert rel_l2(out.stem_intensity, ref) < TOL
+
+
 def test_thickness(ctx):
     p, at = cases.thickness_small()
     out = cb.ThicknessSimulator(ctx=ctx).run(p, at)
