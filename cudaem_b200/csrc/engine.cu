@@ -9,6 +9,7 @@
 //   probe / plane wave -> per slice: row pass, column pass -> post passes ->
 //   FP64 accumulation over configurations -> output.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -257,6 +258,7 @@ struct AtomsDev {
     const int* elem;
     const ElemTable* tables;
     int n_elem;
+    float rmax_all;   // largest cut-off radius over the elements
 };
 
 std::string elem_key(const ms_params& p, int Z)
@@ -310,6 +312,8 @@ AtomsDev upload_atoms(ms_ctx* c, const ms_params& p, const ms_atoms& a)
     CK(cudaMemcpyAsync(t, tabs.data(), sizeof(ElemTable) * tabs.size(), cudaMemcpyHostToDevice, c->stream));
     d.x = x; d.y = y; d.z = z; d.sig = sg; d.occ = oc; d.elem = e; d.tables = t;
     d.n_elem = (int)tabs.size();
+    d.rmax_all = 0.f;
+    for (auto& tb : tabs) d.rmax_all = std::max(d.rmax_all, tb.rmax);
     return d;
 }
 
@@ -322,8 +326,9 @@ struct SpecGroup {
     int S_cap = 0;
     const float *ax = nullptr, *ay = nullptr, *aw = nullptr;
     const int* ae = nullptr;
-    const int64_t* seg = nullptr;
+    const unsigned* seg = nullptr;
     const int* ns_d = nullptr;
+    CellGrid cg;
 };
 
 inline float ord2f(unsigned k)
@@ -388,29 +393,44 @@ SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const
     CK(cudaMemcpyAsync(dnv, nv.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dvmax, vmax.data(), sizeof(float) * nc, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dns, g.ns.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
-    const int nkeys = (int)(nc * (S_cap + 1));
+    // spatial cells: at least the largest cut-off and a quarter of a potential tile (64 x 32 pixels),
+    // so a tile touches at most 7 x 5 cells
+    const double cell = std::max({(double)A.rmax_all, 16.0 * p.lx / p.nx, 16.0 * p.ly / p.ny, 0.25});
+    g.cg.ncx = std::max(1, (int)std::ceil(p.lx / cell));
+    g.cg.ncy = std::max(1, (int)std::ceil(p.ly / cell));
+    g.cg.inv_cell = (float)(1.0 / cell);
+    g.cg.lx = (float)p.lx;
+    g.cg.ly = (float)p.ly;
+    g.cg.wrap = p.pot_wrap ? 1 : 0;
+    const int64_t nkeys64 = nc * (S_cap + 1) * (int64_t)g.cg.ncx * g.cg.ncy;
+    MS_REQUIRE(nkeys64 < (1LL << 31), MS_ERR_UNSUPPORTED, "too many (configuration, slice, cell) bins");
+    const int nkeys = (int)nkeys64;
     const int64_t total = n * nc;
     MS_REQUIRE(total < (1LL << 31), MS_ERR_UNSUPPORTED, "atoms x configurations must stay below 2^31 per group");
     unsigned* keys = (unsigned*)c->buf("sp_keys", sizeof(unsigned) * total);
     unsigned* keys2 = (unsigned*)c->buf("sp_keys2", sizeof(unsigned) * total);
     int* vals = (int*)c->buf("sp_vals", sizeof(int) * total);
     int* vals2 = (int*)c->buf("sp_vals2", sizeof(int) * total);
-    unsigned* counts = (unsigned*)c->buf("sp_counts", sizeof(unsigned) * nkeys);
-    CK(cudaMemsetAsync(counts, 0, sizeof(unsigned) * nkeys, st));
-    launch_assign(zd, n, (int)nc, db, bstride, dnv, dvmax, S_cap, keys, vals, counts, st);
+    unsigned* counts = (unsigned*)c->buf("sp_counts", sizeof(unsigned) * (nkeys + 1));
+    CK(cudaMemsetAsync(counts, 0, sizeof(unsigned) * (nkeys + 1), st));
+    launch_assign(xd, yd, zd, n, (int)nc, db, bstride, dnv, dvmax, S_cap, g.cg, keys, vals, counts, st);
     int end_bit = 1;
     while ((1LL << end_bit) < nkeys) end_bit++;
     size_t tmp_bytes = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, vals2, (int)total, 0, end_bit, st));
     void* tmp = c->buf("sp_sorttmp", tmp_bytes);
     CK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, vals2, (int)total, 0, end_bit, st));
-    int64_t* seg = (int64_t*)c->buf("sp_seg", sizeof(int64_t) * (nkeys + 1));
-    launch_scan_counts(counts, nkeys, seg, st);
+    unsigned* seg = (unsigned*)c->buf("sp_seg", sizeof(unsigned) * (nkeys + 1));
+    size_t scan_bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, seg, nkeys + 1, st));
+    void* scan_tmp = c->buf("sp_scantmp", scan_bytes);
+    CK(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, seg, nkeys + 1, st));
     float* ax = (float*)c->buf("sp_ax", sizeof(float) * total);
     float* ay = (float*)c->buf("sp_ay", sizeof(float) * total);
     float* aw = (float*)c->buf("sp_aw", sizeof(float) * total);
     int* ae = (int*)c->buf("sp_ae", sizeof(int) * total);
-    launch_gather(keys2, vals2, total, n, S_cap, xd, yd, A.occ, A.elem, (float)ph.vr_factor, ax, ay, aw, ae, st);
+    launch_gather(keys2, vals2, total, n, S_cap, g.cg, xd, yd, A.occ, A.elem, (float)ph.vr_factor, ax, ay, aw, ae,
+                  st);
     g.ax = ax; g.ay = ay; g.aw = aw; g.ae = ae; g.seg = seg; g.ns_d = dns;
     return g;
 }
@@ -432,6 +452,10 @@ PotArgs pot_args(const ms_params& p, const Setup& s, const AtomsDev& A, const Sp
     a.dy = (float)s.gc.dy;
     a.lx = (float)p.lx;
     a.ly = (float)p.ly;
+    a.ncx = g.cg.ncx;
+    a.ncy = g.cg.ncy;
+    a.inv_cell = g.cg.inv_cell;
+    a.rmax_all = A.rmax_all;
     a.dx_hi = (float)s.gc.dx;
     a.dx_lo = (float)(s.gc.dx - (double)a.dx_hi);
     a.dy_hi = (float)s.gc.dy;

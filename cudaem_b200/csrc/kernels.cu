@@ -450,7 +450,7 @@ size_t col_smem(int N)
 // projected potential: gen_slice_potential_kernel (device_kernels.cuh:28-47)
 // restructured as atom-culled 64x16 pixel tiles with float4 stores
 // ---------------------------------------------------------------------------
-constexpr int kPotTX = 64, kPotTY = 32, kPotThreads = 256, kPotMaxImg = 4;
+constexpr int kPotTX = 64, kPotTY = 32, kPotThreads = 256;
 constexpr int kPotRowsPerThread = kPotTY / (kPotThreads / (kPotTX / 4));   // 2 rows of 4 pixels
 
 __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
@@ -467,19 +467,10 @@ __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
     return ((c.c3 * d + c.c2) * d + c.c1) * d + c.c0;  // get_value_Cubic_Spline
 }
 
-// Up to four periodic images of an atom kept in registers (no indexed local array).
-struct ImgList {
-    float4 v0, v1, v2, v3;
-    int n = 0;
-    __device__ __forceinline__ void push(float4 v)
-    {
-        if (n == 0) v0 = v;
-        else if (n == 1) v1 = v;
-        else if (n == 2) v2 = v;
-        else if (n == 3) v3 = v;
-        n = min(n + 1, kPotMaxImg);
-    }
-};
+
+constexpr int kPotMaxRanges = 64;
+
+__device__ __forceinline__ int floordiv_i(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
 
 __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
 {
@@ -488,6 +479,9 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
     float4* cand = reinterpret_cast<float4*>(psm + sizeof(ElemTable) * a.n_elem);
     __shared__ int wsum[kPotThreads / 32];
     __shared__ int total_s;
+    __shared__ unsigned r_beg[kPotMaxRanges], r_pre[kPotMaxRanges + 1];
+    __shared__ int r_img[kPotMaxRanges];
+    __shared__ int n_ranges;
 
     const int conf = blockIdx.z;
     const int sl = a.slice0 + blockIdx.y;
@@ -512,34 +506,73 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
             int nv4 = (int)(sizeof(ElemTable) * a.n_elem / 16);
             for (int i = t; i < nv4; i += kPotThreads) dst[i] = src[i];
         }
-        __syncthreads();
-        const int64_t s0 = a.seg[(int64_t)conf * (a.S_cap + 1) + sl];
-        const int64_t s1 = a.seg[(int64_t)conf * (a.S_cap + 1) + sl + 1];
         const float X0 = (float)tx0 * a.dx, X1 = (float)(tx0 + kPotTX - 1) * a.dx;
         const float Y0 = (float)ty0 * a.dy, Y1 = (float)(ty0 + kPotTY - 1) * a.dy;
-        const int lane = t & 31, wid = t >> 5;
-        for (int64_t base = s0; base < s1; base += kPotThreads) {
-            int64_t i = base + t;
-            ImgList im;
-            if (i < s1) {
-                const float xa = a.ax[i], ya = a.ay[i], w = a.aw[i];
-                const int e = a.ae[i];
-                const float rm = el[e].rmax * 1.0001f + 1e-4f;
-#pragma unroll
-                for (int iy = -1; iy <= 1; iy++)
-#pragma unroll
-                    for (int ix = -1; ix <= 1; ix++) {
-                        if (!a.wrap && (ix != 0 || iy != 0)) continue;
-                        // culling only: approximate image position
-                        float xs = xa + (float)ix * a.lx, ys = ya + (float)iy * a.ly;
-                        float dxr = fmaxf(0.f, fmaxf(X0 - xs, xs - X1));
-                        float dyr = fmaxf(0.f, fmaxf(Y0 - ys, ys - Y1));
-                        if (dxr * dxr + dyr * dyr < rm * rm)
-                            im.push(make_float4(xa, ya, w, __int_as_float(e | ((ix + 1) << 8) | ((iy + 1) << 10))));
-                    }
+        if (t == 0) {
+            // Atoms are sorted by (configuration, slice, cell) with cells of a.cell A in a
+            // ncx x ncy grid over the box.  The tile needs the cells its rectangle, grown by the
+            // largest cut-off, touches: one contiguous key range per cell row and periodic image.
+            const float R = a.rmax_all * 1.0001f + 1e-4f;
+            int cx0 = (int)floorf((X0 - R) * a.inv_cell), cx1 = (int)floorf((X1 + R) * a.inv_cell);
+            int cy0 = (int)floorf((Y0 - R) * a.inv_cell), cy1 = (int)floorf((Y1 + R) * a.inv_cell);
+            if (!a.wrap) {
+                cx0 = max(cx0, 0);
+                cy0 = max(cy0, 0);
+                cx1 = min(cx1, a.ncx - 1);
+                cy1 = min(cy1, a.ncy - 1);
             }
-            const int cnt = im.n;
-            // ordered compaction (deterministic: atom order, then image order)
+            const int64_t key_base = ((int64_t)conf * (a.S_cap + 1) + sl) * a.ncx * a.ncy;
+            int nr = 0;
+            unsigned run = 0;
+            r_pre[0] = 0;
+            for (int cy = cy0; cy <= cy1 && nr < kPotMaxRanges; cy++) {
+                const int oy = a.wrap ? floordiv_i(cy, a.ncy) : 0, cyw = cy - oy * a.ncy;
+                int cx = cx0;
+                while (cx <= cx1 && nr < kPotMaxRanges) {
+                    const int ox = a.wrap ? floordiv_i(cx, a.ncx) : 0, cxw = cx - ox * a.ncx;
+                    const int end = min(cx1, (ox + 1) * a.ncx - 1);
+                    const int64_t k0 = key_base + (int64_t)cyw * a.ncx + cxw;
+                    const unsigned b0 = a.seg[k0], b1 = a.seg[k0 + (end - cx) + 1];
+                    if (b1 > b0) {
+                        r_beg[nr] = b0;
+                        r_img[nr] = (ox + 8) | ((oy + 8) << 8);
+                        run += b1 - b0;
+                        r_pre[++nr] = run;
+                    }
+                    cx = end + 1;
+                }
+            }
+            n_ranges = nr;
+        }
+        __syncthreads();
+        const int nr = n_ranges;
+        const unsigned n_atoms = r_pre[nr];
+        const int lane = t & 31, wid = t >> 5;
+        for (unsigned vbase = 0; vbase < n_atoms; vbase += kPotThreads) {
+            const unsigned v = vbase + t;
+            float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
+            int cnt = 0;
+            if (v < n_atoms) {
+                int r = 0;
+                while (r + 1 < nr && r_pre[r + 1] <= v) r++;
+                const unsigned i = r_beg[r] + (v - r_pre[r]);
+                const float xa = a.ax[i], ya = a.ay[i], w = a.aw[i];
+                const int pk = a.ae[i];
+                const int e = pk & 0xFF;
+                // image of the atom seen through this range: the range's image of the atom's
+                // wrapped cell, minus the atom's own wrap count
+                const int ox = (r_img[r] & 0xFF) - 8 - (((pk >> 8) & 15) - 8);
+                const int oy = ((r_img[r] >> 8) & 0xFF) - 8 - (((pk >> 12) & 15) - 8);
+                const float rm = el[e].rmax * 1.0001f + 1e-4f;
+                const float xs = xa + (float)ox * a.lx, ys = ya + (float)oy * a.ly;  // culling only
+                const float dxr = fmaxf(0.f, fmaxf(X0 - xs, xs - X1));
+                const float dyr = fmaxf(0.f, fmaxf(Y0 - ys, ys - Y1));
+                if (dxr * dxr + dyr * dyr < rm * rm) {
+                    cv = make_float4(xa, ya, w, __int_as_float(e | ((ox + 4) << 8) | ((oy + 4) << 12)));
+                    cnt = 1;
+                }
+            }
+            // ordered compaction (deterministic: cell order, then atom order)
             int incl = cnt;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -551,18 +584,15 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
             if (t == 0) {
                 int run = 0;
                 for (int w = 0; w < kPotThreads / 32; w++) {
-                    int v = wsum[w];
+                    int vv = wsum[w];
                     wsum[w] = run;
-                    run += v;
+                    run += vv;
                 }
                 total_s = run;
             }
             __syncthreads();
             const int off = wsum[wid] + incl - cnt;
-            if (cnt > 0) cand[off] = im.v0;
-            if (cnt > 1) cand[off + 1] = im.v1;
-            if (cnt > 2) cand[off + 2] = im.v2;
-            if (cnt > 3) cand[off + 3] = im.v3;
+            if (cnt > 0) cand[off] = cv;
             __syncthreads();
             const int total = total_s;
             for (int q = 0; q < total; q++) {
@@ -573,7 +603,7 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
                 // distance to the image (ox, oy) of the atom: pixel index shifted by -ox*nx, and
                 // i*dx - x formed with dx split in two floats, so the offset is accurate to its own
                 // rounding (the pixel coordinate i*dx alone would carry ~1e-6 A of error)
-                const int ox = ((bits >> 8) & 3) - 1, oy = ((bits >> 10) & 3) - 1;
+                const int ox = ((bits >> 8) & 15) - 4, oy = ((bits >> 12) & 15) - 4;
                 const float fx0 = (float)(tx0 + 4 * px - ox * a.nx), fy0 = (float)(ty0 + py - oy * a.ny);
                 float dx2[4], dy2[RY];
 #pragma unroll
@@ -612,7 +642,7 @@ void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st)
 {
     if (a.nslice <= 0 || n_conf <= 0) return;
     dim3 grid((unsigned)((a.nx / kPotTX) * (a.ny / kPotTY)), (unsigned)a.nslice, (unsigned)n_conf);
-    size_t sm = sizeof(ElemTable) * a.n_elem + sizeof(float4) * kPotThreads * kPotMaxImg;
+    size_t sm = sizeof(ElemTable) * a.n_elem + sizeof(float4) * kPotThreads;
     cudaFuncSetAttribute(k_potential, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_potential<<<grid, kPotThreads, sm, st>>>(a);
     count_launch();
@@ -681,48 +711,72 @@ void launch_zrange(const float* zd, int64_t n, int nconf, unsigned* zmin_bits, u
     check_launch("z range");
 }
 
-__global__ void k_assign(const float* zd, int64_t n, const float* bounds, int bstride, const int* nv,
-                         const float* vmax, int S_cap, unsigned* keys, int* vals, unsigned* counts)
+// Periodic wrap count of a coordinate (0 without wrapping), clamped to the 4 bits it is packed in.
+__device__ __forceinline__ int wrap_count(float x, float L, int wrap)
+{
+    if (!wrap) return 0;
+    int k = (int)floorf(x / L);
+    return min(max(k, -8), 7);
+}
+
+__device__ __forceinline__ int cell_of(float x, float L, const CellGrid& cg, int nc)
+{
+    const int k = wrap_count(x, L, cg.wrap);
+    const int c = (int)floorf((x - (float)k * L) * cg.inv_cell);
+    return min(max(c, 0), nc - 1);
+}
+
+// Key of an atom: (configuration, slice, cell) with the atoms outside every slice in slice slot
+// S_cap; one stable radix sort then groups atoms by slice and, inside a slice, by cell.
+__global__ void k_assign(const float* xd, const float* yd, const float* zd, int64_t n, const float* bounds,
+                         int bstride, const int* nv, const float* vmax, int S_cap, CellGrid cg, unsigned* keys,
+                         int* vals, unsigned* counts)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int ci = blockIdx.y;
-    int s = det_slice_of(zd[(int64_t)ci * n + i], bounds + (int64_t)ci * bstride, nv[ci], vmax[ci]);
-    unsigned key = (unsigned)ci * (unsigned)(S_cap + 1) + (unsigned)(s >= 0 ? s : S_cap);
-    keys[(int64_t)ci * n + i] = key;
-    vals[(int64_t)ci * n + i] = (int)i;
+    const int64_t o = (int64_t)ci * n + i;
+    int s = det_slice_of(zd[o], bounds + (int64_t)ci * bstride, nv[ci], vmax[ci]);
+    const int nc = cg.ncx * cg.ncy;
+    const int cell = (s >= 0) ? cell_of(yd[o], cg.ly, cg, cg.ncy) * cg.ncx + cell_of(xd[o], cg.lx, cg, cg.ncx) : 0;
+    unsigned key = ((unsigned)ci * (unsigned)(S_cap + 1) + (unsigned)(s >= 0 ? s : S_cap)) * (unsigned)nc + cell;
+    keys[o] = key;
+    vals[o] = (int)i;
     atomicAdd(counts + key, 1u);
 }
 
-void launch_assign(const float* zd, int64_t n, int nconf, const float* bounds, int bstride, const int* nv,
-                   const float* vmax, int S_cap, unsigned* keys, int* vals, unsigned* counts, cudaStream_t st)
+void launch_assign(const float* xd, const float* yd, const float* zd, int64_t n, int nconf, const float* bounds,
+                   int bstride, const int* nv, const float* vmax, int S_cap, const CellGrid& cg, unsigned* keys,
+                   int* vals, unsigned* counts, cudaStream_t st)
 {
     dim3 grid((unsigned)((n + 255) / 256), (unsigned)nconf);
-    k_assign<<<grid, 256, 0, st>>>(zd, n, bounds, bstride, nv, vmax, S_cap, keys, vals, counts);
+    k_assign<<<grid, 256, 0, st>>>(xd, yd, zd, n, bounds, bstride, nv, vmax, S_cap, cg, keys, vals, counts);
     count_launch();
     check_launch("slice assignment");
 }
 
-__global__ void k_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const float* xd,
-                         const float* yd, const float* occ, const int* elem, float vr, float* ax, float* ay, float* aw,
-                         int* ae)
+__global__ void k_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, CellGrid cg,
+                         const float* xd, const float* yd, const float* occ, const int* elem, float vr, float* ax,
+                         float* ay, float* aw, int* ae)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     unsigned key = keys[i];
-    int64_t ci = key / (unsigned)(S_cap + 1);
+    int64_t ci = key / ((unsigned)(S_cap + 1) * (unsigned)(cg.ncx * cg.ncy));
     int64_t at = vals[i];
-    ax[i] = xd[ci * n + at];
-    ay[i] = yd[ci * n + at];
+    const float x = xd[ci * n + at], y = yd[ci * n + at];
+    ax[i] = x;
+    ay[i] = y;
     aw[i] = vr * occ[at];
-    ae[i] = elem[at];
+    // element index and the atom's own periodic wrap counts, packed for the potential kernel
+    ae[i] = elem[at] | ((wrap_count(x, cg.lx, cg.wrap) + 8) << 8) | ((wrap_count(y, cg.ly, cg.wrap) + 8) << 12);
 }
 
-void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const float* xd,
-                   const float* yd, const float* occ, const int* elem, float vr_factor, float* ax, float* ay,
-                   float* aw, int* ae, cudaStream_t st)
+void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const CellGrid& cg,
+                   const float* xd, const float* yd, const float* occ, const int* elem, float vr_factor, float* ax,
+                   float* ay, float* aw, int* ae, cudaStream_t st)
 {
-    k_gather<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(keys, vals, total, n, S_cap, xd, yd, occ, elem,
+    k_gather<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(keys, vals, total, n, S_cap, cg, xd, yd, occ, elem,
                                                               vr_factor, ax, ay, aw, ae);
     count_launch();
     check_launch("gather");

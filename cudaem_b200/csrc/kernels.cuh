@@ -63,13 +63,21 @@ struct PassArgs {
     float filt_g2in, filt_g2out;
 };
 
+// Spatial cells of the atom binning: a ncx x ncy grid of square cells of side 1/inv_cell.
+struct CellGrid {
+    int ncx, ncy;
+    float inv_cell;
+    float lx, ly;
+    int wrap;
+};
+
 // Sorted atoms of a group of configurations.
 struct PotArgs {
     const float* ax;
     const float* ay;
     const float* aw;            // Vr_factor * occupancy
-    const int* ae;              // element index
-    const int64_t* seg;         // [n_conf][S_cap + 1] start offsets, seg[.][S_cap] = end
+    const int* ae;              // element index | (wrap count x + 8) << 8 | (wrap count y + 8) << 12
+    const unsigned* seg;        // [n_conf][S_cap + 1][ncx*ncy] + 1 start offsets of each (conf, slice, cell)
     const int* ns;              // slices per configuration
     int S_cap;                  // slice slots per configuration
     int slice0, nslice;         // slices computed by this launch
@@ -80,6 +88,9 @@ struct PotArgs {
     float dx, dy, lx, ly;
     float dx_hi, dx_lo, dy_hi, dy_lo;  // sampling split in two floats: ix*dx - x is formed to float accuracy
     int wrap;
+    int ncx, ncy;
+    float inv_cell;
+    float rmax_all;             // largest cut-off radius of the elements
     const ElemTable* elems;
     int n_elem;
 };
@@ -99,11 +110,12 @@ void launch_displace(const float* x, const float* y, const float* z, const float
                      int nconf, uint64_t seed, int dx, int dy, int dzf, float* xd, float* yd, float* zd,
                      cudaStream_t st);
 void launch_zrange(const float* zd, int64_t n, int nconf, unsigned* zmin_bits, unsigned* zmax_bits, cudaStream_t st);
-void launch_assign(const float* zd, int64_t n, int nconf, const float* bounds, int bstride, const int* nv,
-                   const float* vmax, int S_cap, unsigned* keys, int* vals, unsigned* counts, cudaStream_t st);
-void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const float* xd,
-                   const float* yd, const float* occ, const int* elem, float vr_factor, float* ax, float* ay,
-                   float* aw, int* ae, cudaStream_t st);
+void launch_assign(const float* xd, const float* yd, const float* zd, int64_t n, int nconf, const float* bounds,
+                   int bstride, const int* nv, const float* vmax, int S_cap, const CellGrid& cg, unsigned* keys,
+                   int* vals, unsigned* counts, cudaStream_t st);
+void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const CellGrid& cg,
+                   const float* xd, const float* yd, const float* occ, const int* elem, float vr_factor, float* ax,
+                   float* ay, float* aw, int* ae, cudaStream_t st);
 
 // post-processing
 void launch_detect(const float2* psi, int nwaves, int nx, int ny, float dgx, float dgy, const float* g2in,
