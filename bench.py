@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cbed", choices=["cbed", "stem", "hrtem"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-vs-plain, adjoint and uneven-batch measurements")
     ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
     ap.add_argument("--nconf", type=int, default=0, help="phonon configurations (0: the workload's)")
     return ap.parse_args()
@@ -146,13 +148,12 @@ def cpu_baseline(config: str, p_full, budget_s: float = 20.0):
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
     if config == "cbed":
-        p, at = wl.cbed_si(cells=(16, 16, 10), nconf=1)
-        sample = "1 phonon configuration x 40 slices of the 1024^2 Si CBED workload (16x16x10 cells)"
+        p, at = wl.cbed_si(cells=(16, 16, 60), nconf=1)
+        sample = "1 of the 8 phonon configurations (240 slices) of the 1024^2 Si CBED workload"
         t = time.perf_counter()
         orc.simulate_cbed(p, at)
         dt = time.perf_counter() - t
-        _, _, units_per = 1, 1, 40
-        units = 40
+        units = 240
     elif config == "stem":
         p, at = wl.stem_sto(nconf=1, scan=(2, 1))
         sample = "2 probes x 50 slices of the 1024^2 SrTiO3 STEM workload"
@@ -169,6 +170,94 @@ def cpu_baseline(config: str, p_full, budget_s: float = 20.0):
         units = 40
     return {"value": units / dt, "unit": "probe*slice/s", "cores": threads, "kind": "port", "sample": sample,
             "seconds": dt}
+
+
+def extras(ctx):
+    """The metric's other two legs and the uneven batch, each device-timed through the C ABI:
+    batched STEM against the one-probe-per-launch path, the adjoint against a forward pass,
+    and the 64-instance uneven batch with its completion-latency percentiles."""
+    import ctypes as C
+
+    import torch
+
+    import cudaem_b200 as cb
+    from cudaem_b200 import _abi as abi
+    from cudaem_b200 import workloads as wl
+    L = cb.lib()
+    sim = cb.MulSimulator(ctx=ctx)
+    out = {}
+
+    # batched STEM vs plain (SrTiO3 16x16x25 cells, 1024^2, 50 slices, 22 mrad, ADF 60-200 mrad)
+    def stem_rate(p, at, reps=2):
+        sim.executionSTEM(p, at)
+        best = None
+        for _ in range(reps):
+            sim.executionSTEM(p, at)
+            r = p.scan_nx * p.scan_ny * 50 / (ctx.last_device_ms / 1e3)
+            best = r if best is None else max(best, r)
+        return best, ctx.last_probe_batch
+
+    p, at = wl.stem_sto(nconf=1, scan=(16, 16))
+    batched, B = stem_rate(p, at)
+    q, _ = wl.stem_sto(nconf=1, scan=(4, 2), batch=1)
+    ctx.set_graphs(False)
+    b1, _ = stem_rate(q, at)
+    ctx.set_graphs(True)
+    g, _ = wl.stem_sto(nconf=1, scan=(2, 1))
+    g.exec_mode = abi.MS_EXEC_PLAIN
+    general, _ = stem_rate(g, at, reps=1)
+    out["stem_batched_vs_plain"] = {
+        "workload": "STEM ADF SrTiO3[001] 16x16x25 cells, 1024^2, 50 slices, 200 kV, 22 mrad, one phonon "
+                    "configuration; batched: 16x16 probes in autotuned batches replayed from a CUDA graph; "
+                    "plain: one probe per launch (8 probes), no graph; general scan: the reference's "
+                    "run_STEM_general_simu form, potential regenerated per probe and slice (2 probes)",
+        "unit": "probe*slice/s", "batched": batched, "autotuned_batch": B, "plain": b1, "ratio": batched / b1,
+        "general_scan": general, "ratio_vs_general_scan": batched / general}
+
+    # adjoint vs forward (SrTiO3 10x10x40 cells, 512^2, 80 slices, 16 probes, checkpoints every 8)
+    p, at, xy = wl.adjoint_sto(n_probe=16)
+    V = ctx.projected_potential(p, at, conf=0)
+    rng = np.random.default_rng(7)
+    Vt = (V + 0.01 * np.abs(V) * rng.standard_normal(V.shape)).astype(np.float32)
+    z0 = 0.5 * p.dz
+    T = ctx.stem_forward_potential(p, Vt, z0, xy)
+    Vd = torch.from_numpy(V).cuda()
+    gVd = torch.empty_like(Vd)
+    cp = p.c()
+    xy = np.ascontiguousarray(xy, np.float64)
+    T = np.ascontiguousarray(T, np.float32)
+    I = np.empty((xy.shape[0], p.n_det), np.float32)
+    dptr = xy.ctypes.data_as(C.POINTER(C.c_double))
+    fptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    vptr = C.cast(C.c_void_p(Vd.data_ptr()), C.POINTER(C.c_float))
+    gptr = C.cast(C.c_void_p(gVd.data_ptr()), C.POINTER(C.c_float))
+    loss, g10, g30 = C.c_double(), C.c_double(), C.c_double()
+    fw, bw = [], []
+    for i in range(4):
+        ctx.check(L.ms_stem_forward_potential(ctx.handle, C.byref(cp), vptr, V.shape[0], 1, z0, dptr, xy.shape[0],
+                                              fptr(I)))
+        fw.append(ctx.last_device_ms)
+        ctx.check(L.ms_stem_backward(ctx.handle, C.byref(cp), vptr, V.shape[0], 1, z0, dptr, xy.shape[0], fptr(T),
+                                     C.byref(loss), gptr, C.byref(g10), C.byref(g30)))
+        bw.append(ctx.last_device_ms)
+    f, b = min(fw[1:]), min(bw[1:])
+    out["adjoint"] = {"workload": "differentiable STEM SrTiO3[001] 10x10x40 cells, 512^2, 80 slices, 200 kV, "
+                                  "22 mrad, 16 probes, ADF loss, checkpoints every 8 slices",
+                      "forward_ms": f, "backward_ms": b, "ratio": b / f,
+                      "note": "backward = loss, dL/dV, dL/dC10, dL/dC30 in one call (its own forward sweep included)"}
+
+    # uneven batch: 64 CBED instances, 256^2..2048^2, 10-200 slices, 80-300 kV, 10-30 mrad
+    jobs = wl.uneven_mix(64)
+    sim.executionMany(jobs)
+    outs, lat = sim.executionMany(jobs)
+    units = sum(o.n_slices * max(1, p.pn_nconf) for (p, _), o in zip(jobs, outs))
+    ms = ctx.last_device_ms
+    out["uneven_batch"] = {"workload": "64 CBED instances drawn from seed 42: grids 256^2..2048^2, 10-200 slices "
+                                       "of SrTiO3 or Si, 80-300 kV, 10-30 mrad, one phonon configuration each",
+                           "unit": "probe*slice/s", "value": units / (ms / 1e3), "ms": ms, "probe_slices": units,
+                           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                                          "p99": float(np.percentile(lat, 99)), "max": float(lat.max())}}
+    return out
 
 
 def run_reference(args):
@@ -326,6 +415,8 @@ def run_ours(args):
                          "launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": algo,
                          "kernel_share": {k: v[1] for k, v in prof.items()}},
             "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_extras:
+        line.update(extras(ctx))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.config, p)
     if rank == 0:

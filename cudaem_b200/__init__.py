@@ -255,6 +255,13 @@ class Context:
     def last_launch_count(self) -> int:
         return lib().ms_last_launch_count(self.handle)
 
+    @property
+    def last_probe_batch(self) -> int:
+        return lib().ms_last_probe_batch(self.handle)
+
+    def set_graphs(self, enable: bool) -> None:
+        self.check(lib().ms_set_graphs(self.handle, 1 if enable else 0))
+
     def set_profiling(self, enable: bool) -> None:
         self.check(lib().ms_set_profiling(self.handle, 1 if enable else 0))
 
@@ -377,6 +384,27 @@ class MulSimulator:
         p, a = params.c(), atoms.c()
         self.ctx.check(lib().ms_simulate_stem(self.ctx.handle, C.byref(p), C.byref(a), C.byref(co)))
         return self._finish(o, co)
+
+
+    def executionMany(self, jobs: Sequence[tuple[MultisliceParams, Atoms]]) -> tuple[list[OutputMultiData], np.ndarray]:
+        """Uneven batch (ms_simulate_many): CBED simulations of mixed grids and slice counts in one
+        call.  Returns the outputs and each instance's completion time in ms from the call's start."""
+        n = len(jobs)
+        cp = (abi.ms_params * n)()
+        ca = (abi.ms_atoms * n)()
+        co = (abi.ms_output * n)()
+        outs = []
+        for i, (params, atoms) in enumerate(jobs):
+            C.memmove(C.byref(cp[i]), C.byref(params.c()), C.sizeof(abi.ms_params))
+            ca[i] = atoms.c()
+            o = OutputMultiData(image_intensity=np.empty((params.ny, params.nx), np.float32))
+            co[i].image_intensity = _fptr(o.image_intensity)
+            outs.append(o)
+        lat = np.zeros(n, np.float64)
+        self.ctx.check(lib().ms_simulate_many(self.ctx.handle, n, cp, ca, co, _dptr(lat)))
+        for i in range(n):
+            self._finish(outs[i], co[i])
+        return outs, lat
 
 
 class ThicknessSimulator(MulSimulator):

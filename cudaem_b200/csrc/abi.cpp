@@ -110,6 +110,7 @@ ms_status ms_destroy(ms_ctx* c)
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (auto s : c->side) cudaStreamDestroy(s);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return MS_OK;
@@ -156,6 +157,20 @@ ms_status ms_profile_get(const ms_ctx* c, const char* kernel, int64_t* launches,
 void* ms_get_stream(ms_ctx* c) { return c ? (void*)c->stream : nullptr; }
 double ms_last_device_ms(const ms_ctx* c) { return c ? c->last_ms : 0.0; }
 int64_t ms_last_launch_count(const ms_ctx* c) { return c ? c->last_launches : 0; }
+
+int ms_last_probe_batch(const ms_ctx* c) { return c ? c->last_batch : 0; }
+
+ms_status ms_set_graphs(ms_ctx* c, int enable)
+{
+    if (!c) return MS_ERR_INVALID_ARG;
+    c->use_graphs = enable != 0;
+    if (!c->use_graphs) {
+        cudaSetDevice(c->device);
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        c->drop_graph();
+    }
+    return MS_OK;
+}
 
 ms_status ms_physics(double E0_kV, double* lambda, double* sigma, double* gamma)
 {

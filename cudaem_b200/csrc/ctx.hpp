@@ -28,6 +28,19 @@ struct ms_ctx {
     std::map<int, void*> twiddles;               // inter-level FFT twiddles per transform length
     std::map<std::string, msb::ElemTable> elem_cache;
 
+    // STEM probe-batch graph: one batch's launch sequence (probe, slice loop, detector),
+    // captured once and replayed for every batch whose launch arguments match `graph_key`
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;                    // kernels inside the captured graph
+    };
+    std::map<std::string, Graph> graphs;         // keyed by the launch arguments they bake in
+    bool use_graphs = true;
+    int last_batch = 0;                          // probe batch used by the last STEM call
+    std::vector<cudaStream_t> side;              // streams of the grid groups of an uneven batch
+    std::map<std::string, int> batch_choice;     // autotuned probe batch per grid and slice count
+    void drop_graph();
+
     // per-kernel event timing
     bool profile = false;
     std::vector<cudaEvent_t> ev_pool;

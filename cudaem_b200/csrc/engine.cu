@@ -36,6 +36,7 @@ void* ms_ctx::buf(const std::string& name, size_t bytes)
     if (b.p && b.bytes >= bytes) return b.p;
     if (b.p) {
         cudaStreamSynchronize(stream);
+        drop_graph();   // a captured graph may hold the old address
         cudaFree(b.p);
         b.p = nullptr;
         b.bytes = 0;
@@ -53,9 +54,17 @@ void* ms_ctx::buf(const std::string& name, size_t bytes)
     return p;
 }
 
+void ms_ctx::drop_graph()
+{
+    for (auto& kv : graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+}
+
 void ms_ctx::release_all()
 {
     if (stream) cudaStreamSynchronize(stream);
+    drop_graph();
     for (auto& kv : bufs)
         if (kv.second.p) cudaFree(kv.second.p);
     bufs.clear();
@@ -650,15 +659,132 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
 // STEM (run_STEM_tile_simu, scan_simulator.cuh:11-113; plain form run_STEM_general_simu, :115-183)
 // ---------------------------------------------------------------------------
 namespace {
-int choose_batch(const ms_params& p, int npos, int64_t N)
+// Largest probe batch the memory budget allows (the waves take at most a quarter of free memory).
+int batch_cap(int64_t N)
 {
-    if (p.exec_mode == MS_EXEC_PLAIN) return 1;
-    if (p.probe_batch > 0) return std::min(p.probe_batch, npos);
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     int64_t cap = (int64_t)(fr * 0.25 / (double)(N * 8));
-    int b = (int)std::min<int64_t>(256, std::max<int64_t>(1, cap));
-    return std::min(b, npos);
+    return (int)std::min<int64_t>(256, std::max<int64_t>(1, cap));
+}
+
+// Probe-batch autotuner: times one probe generation and two slice steps (row + column pass)
+// for each candidate batch size on the call's own grid and potentials, and keeps the size
+// with the highest probe*slice rate.  The choice is cached in the context per grid, slice
+// count and cap.  Candidates are powers of two from 32 to 256 within the memory cap.
+int autotune_batch(ms_ctx* c, const ms_params& p, const Setup& s, const PassArgs& base, const WaveInfo& w0, int S,
+                   int npos, int cap)
+{
+    const int hi = std::min(cap, npos);
+    std::vector<int> cand;
+    for (int b = 32; b <= 256; b *= 2)
+        if (b <= hi) cand.push_back(b);
+    if (cand.empty()) return std::max(1, hi);
+    if (cand.size() == 1 || c->profile) return cand.back();
+    char key[96];
+    std::snprintf(key, sizeof(key), "%d,%d,%d,%d", p.nx, p.ny, std::min(S, 2), hi);
+    auto it = c->batch_choice.find(key);
+    if (it != c->batch_choice.end()) return it->second;
+    cudaStream_t st = c->stream;
+    const int bmax = cand.back();
+    std::vector<WaveInfo> wv((size_t)bmax, w0);
+    WaveInfo* dwv = (WaveInfo*)c->buf("waves_tune", sizeof(WaveInfo) * bmax);
+    CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * bmax, cudaMemcpyHostToDevice, st));
+    float2* psi = (float2*)c->buf("psi", sizeof(float2) * s.N * bmax);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int best = cand.back();
+    double best_rate = -1.0;
+    PassArgs pa = base;
+    pa.psi = psi;
+    pa.waves = dwv;
+    for (int rep = 0; rep < 2; rep++) {   // the first round warms up every candidate
+        for (int b : cand) {
+            CK(cudaEventRecord(e0, st));
+            pa.tw = s.tw_y;
+            launch_col(p.ny, COL_PROBE_INV, pa, b, p.nx, st);
+            for (int sl = 0; sl < 2; sl++) {
+                pa.slice = std::min(sl, S - 1);
+                pa.tw = s.tw_x;
+                launch_row(p.nx, ROW_INV_T_FWD, pa, b, p.ny, st);
+                pa.tw = s.tw_y;
+                launch_col(p.ny, COL_STEP, pa, b, p.nx, st);
+            }
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            // a batch does one probe generation per S slice steps
+            const double rate = (double)b * 2.0 / (ms * (1.0 + 0.5 / std::max(S, 1)));
+            if (rep == 1 && rate > best_rate) {
+                best_rate = rate;
+                best = b;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->batch_choice[key] = best;
+    return best;
+}
+
+// Launch arguments that a captured batch graph bakes in, as a byte string.
+std::string graph_key_of(const PassArgs& pa, int nb, int S, int nblk, int ndet, const void* partial,
+                         const void* Iw, const void* img, const void* thr, int npos)
+{
+    std::string k((const char*)&pa, sizeof(PassArgs));
+    const int ints[5] = {nb, S, nblk, ndet, npos};
+    const void* ptrs[4] = {partial, Iw, img, thr};
+    k.append((const char*)ints, sizeof(ints));
+    k.append((const char*)ptrs, sizeof(ptrs));
+    return k;
+}
+
+// Runs `body` (launches only) on the context stream through a cached CUDA graph: captured on
+// first use or when `key` changes, replayed otherwise.  Falls back to direct launches while
+// profiling (per-launch events), on the legacy default stream, or when the stream is already
+// being captured by the caller.
+template <class F>
+void run_graphed(ms_ctx* c, const std::string& key, F&& body)
+{
+    cudaStream_t st = c->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    bool ok = c->use_graphs && !c->profile && st != nullptr && st != cudaStreamLegacy &&
+              st != cudaStreamPerThread && cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
+              cs == cudaStreamCaptureStatusNone;
+    if (!ok) {
+        body();
+        return;
+    }
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) {
+        if (c->graphs.size() >= 4) c->drop_graph();   // full batches, the last partial batch, ...
+        const int64_t l0 = kernel_launches();
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            body();
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(st, &g));
+        cudaGraphExec_t ge = nullptr;
+        cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        ms_ctx::Graph gr;
+        gr.exec = ge;
+        gr.launches = kernel_launches() - l0;
+        add_kernel_launches(-gr.launches);   // captured, not run
+        it = c->graphs.emplace(key, gr).first;
+    }
+    CK(cudaGraphLaunch(it->second.exec, st));
+    add_kernel_launches(it->second.launches);
 }
 }  // namespace
 
@@ -687,12 +813,12 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
     CK(cudaMemcpyAsync(dthr, thr.data(), sizeof(float) * 2 * ndet, cudaMemcpyHostToDevice, st));
     double* img = (double*)c->buf("stem_acc", sizeof(double) * ndet * npos);
     CK(cudaMemsetAsync(img, 0, sizeof(double) * ndet * npos, st));
-    const int B = choose_batch(p, npos, N);
     const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
-    double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
-    double* Iw = (double*)c->buf("det_I", sizeof(double) * B * ndet);
-    std::vector<WaveInfo> wv((size_t)B);
-    std::vector<double> Ih((size_t)B * ndet);
+    const int cap = plain ? 1 : (p.probe_batch > 0 ? std::min(p.probe_batch, npos) : batch_cap(N));
+    int B = plain ? 1 : std::min(cap, npos);
+    bool tuned = plain || p.probe_batch > 0;
+    std::vector<WaveInfo> wv((size_t)npos);
+    std::vector<double> Ih((size_t)ndet);
     for (int conf : cs.confs) {
         SpecGroup g = build_specimen(c, p, A, std::vector<int>{conf}, s.ph);
         const int S = g.ns[0];
@@ -705,32 +831,62 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
         } else {
             sV = (float*)c->buf("sV1", sizeof(float) * N);
         }
+        // every scan position of this configuration, uploaded once (run_STEM_tile_simu's tile loop,
+        // scan_simulator.cuh:57-104, without a host round trip per batch)
+        for (int ip = 0; ip < npos; ip++) {
+            const int ix = ip % p.scan_nx, iy = ip / p.scan_nx;
+            wv[ip].px = p.scan_x0 + ix * p.scan_dx;
+            wv[ip].py = p.scan_y0 + iy * p.scan_dy;
+            wv[ip].cc10 = cc10;
+            wv[ip].conf_slot = 0;
+            wv[ip].n_slices = S;
+            wv[ip].weight = (float)cs.weight;
+            wv[ip].pos = ip;
+        }
+        WaveInfo* dwv_all = (WaveInfo*)c->buf("waves_all", sizeof(WaveInfo) * npos);
+        CK(cudaMemcpyAsync(dwv_all, wv.data(), sizeof(WaveInfo) * npos, cudaMemcpyHostToDevice, st));
+        if (!tuned) {
+            PassArgs base = pass_args(s, nullptr, nullptr, sV, slot, cond);
+            B = autotune_batch(c, p, s, base, wv[0], S, npos, cap);
+            tuned = true;
+        }
+        WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * B);
+        float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * B);
+        double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
+        double* Iw = (double*)c->buf("det_I", sizeof(double) * B * ndet);
         for (int start = 0; start < npos; start += B) {
             const int nb = std::min(B, npos - start);
-            for (int i = 0; i < nb; i++) {
-                int ip = start + i, ix = ip % p.scan_nx, iy = ip / p.scan_nx;
-                wv[i].px = p.scan_x0 + ix * p.scan_dx;
-                wv[i].py = p.scan_y0 + iy * p.scan_dy;
-                wv[i].cc10 = cc10;
-                wv[i].conf_slot = 0;
-                wv[i].n_slices = S;
-                wv[i].weight = (float)cs.weight;
-                wv[i].pos = ip;
-            }
-            WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * B);
-            CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nb, cudaMemcpyHostToDevice, st));
-            float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * B);
+            CK(cudaMemcpyAsync(dwv, dwv_all + start, sizeof(WaveInfo) * nb, cudaMemcpyDeviceToDevice, st));
             PassArgs pa = pass_args(s, psi, dwv, sV, plain ? 0 : slot, cond);
+            if (!plain) {
+                auto body = [&] {
+                    PassArgs q = pa;
+                    q.tw = s.tw_y;
+                    run_col(c, p.ny, COL_PROBE_INV, q, nb, p.nx, st);
+                    for (int sl = 0; sl < S; sl++) {
+                        q.slice = sl;
+                        q.tw = s.tw_x;
+                        run_row(c, p.nx, ROW_INV_T_FWD, q, nb, p.ny, st);
+                        q.tw = s.tw_y;
+                        run_col(c, p.ny, COL_STEP, q, nb, p.nx, st);
+                    }
+                    launch_detect(psi, nb, p.nx, p.ny, s.gd.dgx_f, s.gd.dgy_f, dthr, dthr + ndet, ndet, partial, nblk,
+                                  st);
+                    launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw, img, npos, 1, st);
+                };
+                run_graphed(c, graph_key_of(pa, nb, S, nblk, ndet, partial, Iw, img, dthr, npos), body);
+                continue;
+            }
+            // plain form (run_STEM_general_simu): one probe per launch, the slice potential
+            // regenerated for every probe and slice (transmit -> generate_potential_single_slice,
+            // transmission_function.cuh:107-111), a blocking read of the probe's detector sums
+            // (integrated_intensity, wave_function.cuh:135-146)
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_PROBE_INV, pa, nb, p.nx, st);
             for (int sl = 0; sl < S; sl++) {
                 pa.slice = sl;
-                if (plain) {
-                    // the reference's general scan regenerates the slice potential for every probe
-                    // (transmit -> generate_potential_single_slice, transmission_function.cuh:107-111)
-                    run_potential(c, pot_args(p, s, A, g, sV, 0, sl, 1, sl), 1, st);
-                    pa.sV_slice_base = sl;
-                }
+                run_potential(c, pot_args(p, s, A, g, sV, 0, sl, 1, sl), 1, st);
+                pa.sV_slice_base = sl;
                 pa.tw = s.tw_x;
                 run_row(c, p.nx, ROW_INV_T_FWD, pa, nb, p.ny, st);
                 pa.tw = s.tw_y;
@@ -738,13 +894,11 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
             }
             launch_detect(psi, nb, p.nx, p.ny, s.gd.dgx_f, s.gd.dgy_f, dthr, dthr + ndet, ndet, partial, nblk, st);
             launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw, img, npos, 1, st);
-            if (plain) {
-                // integrated_intensity: a blocking read of the probe's detector sums (wave_function.cuh:135-146)
-                CK(cudaMemcpyAsync(Ih.data(), Iw, sizeof(double) * nb * ndet, cudaMemcpyDeviceToHost, st));
-            }
-            CK(cudaStreamSynchronize(st));  // the host wave table is refilled by the next batch
+            CK(cudaMemcpyAsync(Ih.data(), Iw, sizeof(double) * nb * ndet, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
         }
     }
+    c->last_batch = B;
     float* o = (float*)c->buf("stem_out", sizeof(float) * ndet * npos);
     launch_d2f(img, (int64_t)ndet * npos, o, st);
     copy_out(c, out->stem_intensity, o, (int64_t)ndet * npos, out->on_device);
@@ -793,8 +947,6 @@ void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* 
                "thickness_frames holds fewer than n_slices*ny*nx floats");
     float* frames = (float*)c->buf("frames", sizeof(float) * N * nf);
     CK(cudaMemsetAsync(frames, 0, sizeof(float) * N * nf, st));
-    float* dthr = nullptr;
-    (void)dthr;
     const float g2in = g2_threshold(p.det_inner[p.thick_det], s.ph.lambda);
     const float g2out = g2_threshold(p.det_outer[p.thick_det], s.ph.lambda);
     for (int conf : cs.confs) {
@@ -949,15 +1101,423 @@ void sim_stem_forward_potential(ms_ctx* c, const ms_params& p, const float* V, i
     tm.stop();
 }
 
-void sim_stem_backward(ms_ctx*, const ms_params&, const float*, int, int, double, const double*, int, const float*,
-                       double*, float*, double*, double*)
+// ---------------------------------------------------------------------------
+// Adjoint of the STEM forward on caller potentials (or_stem_backward restated on the fused
+// passes).  Per probe batch:
+//   forward sweep, storing the wave every k slices (and, for the last segment, the
+//   transmitted real-space waves x_s = t_s psi_s directly) -> detector sums -> residuals ->
+//   seed lambda = sum_d 4 (I_d - T_d) Psi [annulus d] and its inverse column transform ->
+//   per segment, last to first: recompute x_s from the segment's checkpoint, then sweep the
+//   adjoint back through the segment (row adjoint with the dL/dV update, conj(P) column step)
+//   -> at slice 0 the lens-phase gradient sums.
+// ---------------------------------------------------------------------------
+void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int on_dev, double z_init,
+                       const double* xy, int np, const float* target, double* loss, float* dV, double* dC10,
+                       double* dC30)
 {
-    throw MsError(MS_ERR_UNSUPPORTED, "the adjoint is not built into this library yet");
+    validate_params(p);
+    MS_REQUIRE(V && xy && target && S >= 1 && np >= 1 && p.n_det >= 1, MS_ERR_INVALID_ARG, "bad arguments");
+    MS_REQUIRE(p.ckpt_interval >= 1, MS_ERR_INVALID_ARG, "ckpt_interval must be >= 1");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    Timer tm(c);
+    Setup s = make_setup(c, p);
+    const int64_t N = s.N, slot = (int64_t)S * N;
+    LensDev cond = lens_dev(lens_coef(p.cond_lens, s.ph.lambda, 0.0));
+    const float* sV = V;
+    if (!on_dev) {
+        float* d = (float*)c->buf("sV", sizeof(float) * slot);
+        CK(cudaMemcpyAsync(d, V, sizeof(float) * slot, cudaMemcpyHostToDevice, st));
+        sV = d;
+    }
+    const int ndet = p.n_det;
+    std::vector<float> thr(2 * ndet);
+    for (int d = 0; d < ndet; d++) {
+        thr[d] = g2_threshold(p.det_inner[d], s.ph.lambda);
+        thr[ndet + d] = g2_threshold(p.det_outer[d], s.ph.lambda);
+    }
+    float* dthr = (float*)c->buf("det_thr", sizeof(float) * 2 * ndet);
+    CK(cudaMemcpyAsync(dthr, thr.data(), sizeof(float) * 2 * ndet, cudaMemcpyHostToDevice, st));
+    float* dtgt = (float*)c->buf("adj_target", sizeof(float) * np * ndet);
+    CK(cudaMemcpyAsync(dtgt, target, sizeof(float) * np * ndet, cudaMemcpyHostToDevice, st));
+
+    const int k = p.ckpt_interval;
+    const int nseg = (S + k - 1) / k;
+    // probes per batch: adjoint wave, forward wave, one segment of transmitted waves and the
+    // checkpoints must fit the memory budget
+    const size_t per_wave = (size_t)N * 8 * (2 + (size_t)k + (size_t)(nseg - 1));
+    int B = p.probe_batch > 0 ? p.probe_batch : 256;
+    B = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, free_budget() / per_wave));
+    B = std::min(B, np);
+    const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
+    const int tiles = col_tiles(p.ny, p.nx);
+    float2* adj = (float2*)c->buf("adj_psi", sizeof(float2) * N * B);
+    float2* xseg = (float2*)c->buf("adj_xseg", sizeof(float2) * N * B * k);
+    float2* ckpt = nseg > 1 ? (float2*)c->buf("adj_ckpt", sizeof(float2) * N * B * (nseg - 1)) : nullptr;
+    float* gV = on_dev ? dV : (float*)c->buf("adj_dV", sizeof(float) * slot);
+    double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
+    double* Iw = (double*)c->buf("det_I", sizeof(double) * B * ndet);
+    double* resid = (double*)c->buf("adj_resid", sizeof(double) * B * ndet);
+    double* sq = (double*)c->buf("adj_sq", sizeof(double) * np * ndet);
+    double* chi_part = (double*)c->buf("adj_chi_part", sizeof(double) * B * tiles * 2);
+    double* chi_acc = (double*)c->buf("adj_chi", sizeof(double) * 2);
+    CK(cudaMemsetAsync(gV, 0, sizeof(float) * slot, st));
+    CK(cudaMemsetAsync(chi_acc, 0, sizeof(double) * 2, st));
+    const double cc10 = gate_coef(-kPi * (p.cond_lens.c10 + z_init) * s.ph.lambda);
+    std::vector<WaveInfo> wv((size_t)B);
+    for (int start = 0; start < np; start += B) {
+        const int nb = std::min(B, np - start);
+        const int64_t wstride = (int64_t)nb * N;   // one slice of the batch in xseg / ckpt
+        for (int i = 0; i < nb; i++) {
+            wv[i].px = xy[2 * (start + i)];
+            wv[i].py = xy[2 * (start + i) + 1];
+            wv[i].cc10 = cc10;
+            wv[i].conf_slot = 0;
+            wv[i].n_slices = S;
+            wv[i].weight = 1.0f;
+            wv[i].pos = start + i;
+        }
+        WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * B);
+        CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nb, cudaMemcpyHostToDevice, st));
+        PassArgs pa = pass_args(s, adj, dwv, sV, slot, cond);
+        pa.det_thr = dthr;
+        pa.ndet = ndet;
+        pa.resid = resid;
+        pa.chi_part = chi_part;
+        // forward sweep with checkpoints
+        pa.tw = s.tw_y;
+        run_col(c, p.ny, COL_PROBE_INV, pa, nb, p.nx, st);
+        const int last0 = (nseg - 1) * k;
+        for (int sl = 0; sl < S; sl++) {
+            if (sl < last0 && sl % k == 0)
+                CK(cudaMemcpyAsync(ckpt + (int64_t)(sl / k) * wstride, adj, sizeof(float2) * wstride,
+                                   cudaMemcpyDeviceToDevice, st));
+            pa.slice = sl;
+            pa.flags = sl >= last0 ? PF_STORE_X : 0;
+            pa.xs = xseg + (int64_t)(sl - last0) * wstride;
+            pa.tw = s.tw_x;
+            run_row(c, p.nx, ROW_INV_T_FWD, pa, nb, p.ny, st);
+            pa.flags = 0;
+            pa.tw = s.tw_y;
+            run_col(c, p.ny, COL_STEP, pa, nb, p.nx, st);
+        }
+        launch_detect(adj, nb, p.nx, p.ny, s.gd.dgx_f, s.gd.dgy_f, dthr, dthr + ndet, ndet, partial, nblk, st);
+        launch_det_finalize(partial, nb, nblk, ndet, dwv, Iw, nullptr, 0, 0, st);
+        launch_resid(Iw, dtgt + (int64_t)start * ndet, nb * ndet, resid, sq + (int64_t)start * ndet, st);
+        pa.tw = s.tw_y;
+        run_col(c, p.ny, COL_SEED, pa, nb, p.nx, st);
+        for (int seg = nseg - 1; seg >= 0; seg--) {
+            const int c0 = seg * k, c1 = std::min(S, c0 + k);
+            if (seg != nseg - 1) {
+                // recompute the segment's transmitted waves in place on its checkpoint
+                PassArgs pr = pa;
+                pr.psi = ckpt + (int64_t)seg * wstride;
+                for (int sl = c0; sl < c1; sl++) {
+                    pr.slice = sl;
+                    pr.flags = PF_STORE_X;
+                    pr.xs = xseg + (int64_t)(sl - c0) * wstride;
+                    pr.tw = s.tw_x;
+                    run_row(c, p.nx, ROW_INV_T_FWD, pr, nb, p.ny, st);
+                    if (sl < c1 - 1) {
+                        pr.flags = 0;
+                        pr.tw = s.tw_y;
+                        run_col(c, p.ny, COL_STEP, pr, nb, p.nx, st);
+                    }
+                }
+            }
+            for (int i = c1 - 1; i >= c0; i--) {
+                pa.slice = i;
+                pa.flags = 0;
+                pa.xs = xseg + (int64_t)(i - c0) * wstride;
+                pa.dV = gV + (int64_t)i * N;
+                pa.tw = s.tw_x;
+                run_row(c, p.nx, ROW_ADJ, pa, nb, p.ny, st);
+                pa.tw = s.tw_y;
+                if (i > 0) {
+                    pa.slice = i - 1;
+                    pa.flags = PF_CONJ_PROP | PF_PROP_ALWAYS;
+                    run_col(c, p.ny, COL_STEP, pa, nb, p.nx, st);
+                } else {
+                    run_col(c, p.ny, COL_GRAD_PROBE, pa, nb, p.nx, st);
+                    launch_chi_finalize(chi_part, nb, tiles, chi_acc, st);
+                }
+            }
+        }
+        CK(cudaStreamSynchronize(st));  // the host wave table is refilled by the next batch
+    }
+    if (!on_dev) CK(cudaMemcpyAsync(dV, gV, sizeof(float) * slot, cudaMemcpyDeviceToHost, st));
+    std::vector<double> hsq((size_t)np * ndet);
+    double hchi[2];
+    CK(cudaMemcpyAsync(hsq.data(), sq, sizeof(double) * np * ndet, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hchi, chi_acc, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+    tm.stop();
+    double L = 0.0;
+    for (double v : hsq) L += v;
+    if (loss) *loss = L;
+    const double lam = s.ph.lambda;
+    if (dC10) *dC10 = -kPi * lam * hchi[0];
+    if (dC30) *dC30 = -kPi * lam * lam * lam / 2.0 * hchi[1];
 }
 
-void sim_many(ms_ctx*, int, const ms_params*, const ms_atoms*, ms_output*, double*)
+// ---------------------------------------------------------------------------
+// Uneven batch: n independent CBED simulations of mixed grid sizes, slice counts, beam
+// energies and probes in one call.  Instances with the same grid share every pass launch:
+// one row pass and one column pass per slice cover the waves of all instances of that
+// grid that still have slices left, each wave reading its own instance's potential store
+// and propagator table through its wave descriptor.  Grid groups run on their own streams
+// and interleave slice by slice; an instance's pattern is accumulated and written as soon
+// as its last slice is done, and an event records that completion.
+// ---------------------------------------------------------------------------
+namespace {
+cudaStream_t side_stream(ms_ctx* c, size_t i)
 {
-    throw MsError(MS_ERR_UNSUPPORTED, "uneven batches are not built into this library yet");
+    while (c->side.size() <= i) {
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        c->side.push_back(s);
+    }
+    return c->side[i];
+}
+}  // namespace
+
+void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_output* outs, double* lat)
+{
+    for (int i = 0; i < n; i++) {
+        validate_params(ps[i]);
+        validate_atoms(ps[i], &as[i]);
+        MS_REQUIRE(ps[i].simulation_type == MS_SIM_CBED, MS_ERR_UNSUPPORTED,
+                   "uneven batches run CBED simulations (simulation_type = MS_SIM_CBED)");
+        MS_REQUIRE(ps[i].data_record == MS_RECORD_INTENSITY, MS_ERR_UNSUPPORTED,
+                   "uneven batches record intensities");
+        MS_REQUIRE(outs[i].image_intensity != nullptr, MS_ERR_INVALID_ARG, "image_intensity is NULL");
+    }
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    const bool prof = c->profile;
+    c->profile = false;   // per-launch events live on the context stream; groups run on side streams
+    struct Restore {
+        ms_ctx* c;
+        bool v;
+        ~Restore() { c->profile = v; }
+    } restore{c, prof};
+    Timer tm(c);
+    std::vector<cudaEvent_t> done((size_t)n, nullptr);
+    struct EvFree {
+        std::vector<cudaEvent_t>* v;
+        ~EvFree()
+        {
+            for (auto e : *v)
+                if (e) cudaEventDestroy(e);
+        }
+    } evfree{&done};
+    for (int i = 0; i < n; i++) CK(cudaEventCreate(&done[i]));
+
+    // per instance: physics, propagator table, potential store
+    struct Inst {
+        int nconf = 0;
+        std::vector<WaveInfo> waves;
+        int S_max = 0;
+        GridDev gd;
+        LensDev cond;
+        float* sV = nullptr;
+        float2* prop = nullptr;
+        float* out = nullptr;
+    };
+    std::vector<Inst> in((size_t)n);
+    // memory plan: instances whose stores do not fit together run in successive rounds
+    std::vector<size_t> need((size_t)n);
+    for (int i = 0; i < n; i++) {
+        const int64_t N = (int64_t)ps[i].nx * ps[i].ny;
+        const ConfSet cs = conf_set(ps[i]);
+        need[i] = (size_t)N * (4 * (size_t)estimate_slices(ps[i], as[i]) * cs.confs.size() + 8 + 4 + 8 * cs.confs.size());
+    }
+    int r0 = 0;
+    while (r0 < n) {
+        size_t budget = free_budget(), used = 0;
+        int r1 = r0;
+        while (r1 < n && (r1 == r0 || used + need[r1] <= budget)) used += need[r1++];
+        // ---- phase 1 (context stream): specimens, potentials, propagators
+        for (int i = r0; i < r1; i++) {
+            const ms_params& p = ps[i];
+            Inst& I = in[i];
+            const Physics ph = physics_of(p.E0, p.theta);
+            const GridConst gc = grid_of(p, ph);
+            const int64_t N = (int64_t)p.nx * p.ny;
+            Setup s0;
+            s0.ph = ph;
+            s0.gc = gc;
+            s0.N = N;
+            s0.gd.nx = p.nx;
+            s0.gd.ny = p.ny;
+            s0.gd.dgx_f = gc.dgx_f;
+            s0.gd.dgy_f = gc.dgy_f;
+            s0.gd.dgx = gc.dgx;
+            s0.gd.dgy = gc.dgy;
+            s0.gd.gl2_f = (float)gc.gl2;
+            s0.gd.alpha_f = (float)gc.alpha;
+            s0.gd.bwl = p.bwl ? 1 : 0;
+            s0.gd.inv_n = 1.0f / (float)N;
+            I.gd = s0.gd;
+            I.cond = lens_dev(lens_coef(p.cond_lens, ph.lambda, 0.0));
+            AtomsDev A = upload_atoms(c, p, as[i]);
+            ConfSet cs = conf_set(p);
+            SpecGroup g = build_specimen(c, p, A, cs.confs, ph);
+            I.nconf = g.nconf;
+            const int64_t slot = (int64_t)g.S_cap * N;
+            I.sV = (float*)c->buf("many_sV_" + std::to_string(i), sizeof(float) * slot * g.nconf);
+            run_potential(c, pot_args(p, s0, A, g, I.sV, slot, 0, g.S_cap, 0), g.nconf, st);
+            I.prop = (float2*)c->buf("many_prop_" + std::to_string(i), sizeof(float2) * N);
+            launch_prop_table(p.nx, p.ny, gc.dgx, gc.dgy, gc.g0x, gc.g0y, gc.prop_w, gc.alpha, gc.gl2, p.bwl ? 1 : 0,
+                              I.prop, st);
+            I.out = (float*)c->buf("many_out_" + std::to_string(i), sizeof(float) * N);
+            I.waves.assign((size_t)g.nconf, WaveInfo());
+            I.S_max = 0;
+            for (int k = 0; k < g.nconf; k++) {
+                WaveInfo& w = I.waves[k];
+                w.px = p.iw_x;
+                w.py = p.iw_y;
+                w.cc10 = gate_coef(-kPi * (p.cond_lens.c10 + g.z_init[k]) * ph.lambda);
+                w.conf_slot = 0;
+                w.n_slices = g.ns[k];
+                w.weight = (float)cs.weight;
+                w.pos = i;
+                w.sV = I.sV + (int64_t)k * slot;
+                w.prop = I.prop;
+                I.S_max = std::max(I.S_max, g.ns[k]);
+            }
+        }
+        // ---- phase 2: grid groups on side streams, interleaved slice by slice
+        struct Group {
+            int nx, ny;
+            std::vector<int> inst;      // instances, longest first
+            std::vector<int> off;       // first wave of each instance
+            std::vector<WaveInfo> waves;
+            WaveInfo* dwv = nullptr;
+            float2* psi = nullptr;
+            double* acc = nullptr;
+            cudaStream_t s = nullptr;
+            int S_max = 0;
+        };
+        std::vector<Group> groups;
+        for (int i = r0; i < r1; i++) {
+            size_t gi = 0;
+            while (gi < groups.size() && !(groups[gi].nx == ps[i].nx && groups[gi].ny == ps[i].ny)) gi++;
+            if (gi == groups.size()) {
+                groups.emplace_back();
+                groups.back().nx = ps[i].nx;
+                groups.back().ny = ps[i].ny;
+            }
+            groups[gi].inst.push_back(i);
+        }
+        // tables every group reads, made before the groups fork off the context stream
+        if (!c->exptab) make_setup(c, ps[r0]);
+        const float2* ex = (const float2*)c->exptab;
+        for (Group& G : groups) {
+            twiddles(c, G.nx);
+            twiddles(c, G.ny);
+        }
+        cudaEvent_t fork = c->prof_event();
+        CK(cudaEventRecord(fork, st));
+        for (size_t gi = 0; gi < groups.size(); gi++) {
+            Group& G = groups[gi];
+            std::stable_sort(G.inst.begin(), G.inst.end(), [&](int a, int b) { return in[a].S_max > in[b].S_max; });
+            for (int i : G.inst) {
+                G.off.push_back((int)G.waves.size());
+                G.waves.insert(G.waves.end(), in[i].waves.begin(), in[i].waves.end());
+            }
+            G.S_max = in[G.inst.front()].S_max;
+            const int64_t N = (int64_t)G.nx * G.ny;
+            const std::string tag = std::to_string(G.nx) + "x" + std::to_string(G.ny);
+            G.dwv = (WaveInfo*)c->buf("many_waves_" + tag, sizeof(WaveInfo) * G.waves.size());
+            G.psi = (float2*)c->buf("many_psi_" + tag, sizeof(float2) * N * G.waves.size());
+            G.acc = (double*)c->buf("many_acc_" + tag, sizeof(double) * N);
+            G.s = side_stream(c, gi);
+            CK(cudaStreamWaitEvent(G.s, fork, 0));
+            CK(cudaMemcpyAsync(G.dwv, G.waves.data(), sizeof(WaveInfo) * G.waves.size(), cudaMemcpyHostToDevice, G.s));
+        }
+        // probes, per instance (each has its own lens, grid and wavelength)
+        for (Group& G : groups) {
+            for (size_t k = 0; k < G.inst.size(); k++) {
+                const Inst& I = in[G.inst[k]];
+                PassArgs pa;
+                std::memset(&pa, 0, sizeof(pa));
+                pa.psi = G.psi + (int64_t)G.off[k] * G.nx * G.ny;
+                pa.waves = G.dwv + G.off[k];
+                pa.grid = I.gd;
+                pa.lens = I.cond;
+                pa.tw = twiddles(c, G.ny);
+                launch_col(G.ny, COL_PROBE_INV, pa, I.nconf, G.nx, G.s);
+            }
+        }
+        int S_all = 0;
+        for (Group& G : groups) S_all = std::max(S_all, G.S_max);
+        std::vector<size_t> next((size_t)groups.size(), 0);   // next instance (in S order) to finish, per group
+        for (int sl = 0; sl < S_all; sl++) {
+            for (size_t gi = 0; gi < groups.size(); gi++) {
+                Group& G = groups[gi];
+                if (sl >= G.S_max) continue;
+                // active waves: instances with slices left form a prefix
+                size_t ki = 0;
+                while (ki < G.inst.size() && in[G.inst[ki]].S_max > sl) ki++;
+                const int nact = ki < G.inst.size() ? G.off[ki] : (int)G.waves.size();
+                PassArgs pa;
+                std::memset(&pa, 0, sizeof(pa));
+                pa.psi = G.psi;
+                pa.waves = G.dwv;
+                pa.slice = sl;
+                pa.exptab = ex;
+                pa.grid = in[G.inst.front()].gd;
+                pa.tw = twiddles(c, G.nx);
+                launch_row(G.nx, ROW_INV_T_FWD, pa, nact, G.ny, G.s);
+                pa.tw = twiddles(c, G.ny);
+                launch_col(G.ny, COL_STEP, pa, nact, G.nx, G.s);
+                // instances whose last slice this was: pattern out, completion event
+                while (next[gi] < G.inst.size() && in[G.inst[G.inst.size() - 1 - next[gi]]].S_max == sl + 1) {
+                    const size_t kk = G.inst.size() - 1 - next[gi];
+                    const int i = G.inst[kk];
+                    const int64_t N = (int64_t)G.nx * G.ny;
+                    launch_acc_abs2(G.psi + (int64_t)G.off[kk] * N, in[i].nconf, G.dwv + G.off[kk], N, G.acc, 1, G.s);
+                    launch_emit(G.acc, G.nx, G.ny, 1, in[i].out, G.s);
+                    CK(cudaEventRecord(done[i], G.s));
+                    next[gi]++;
+                }
+            }
+        }
+        for (Group& G : groups) {
+            cudaEvent_t j = c->prof_event();
+            CK(cudaEventRecord(j, G.s));
+            CK(cudaStreamWaitEvent(st, j, 0));
+        }
+        for (int i = r0; i < r1; i++) copy_out(c, outs[i].image_intensity, in[i].out, (int64_t)ps[i].nx * ps[i].ny,
+                                               outs[i].on_device);
+        CK(cudaStreamSynchronize(st));
+        c->ev_used = 0;
+        // a later round reuses buffer names; drop this round's stores
+        for (int i = r0; i < r1; i++) {
+            for (const char* nm : {"many_sV_", "many_prop_", "many_out_"}) {
+                auto it = c->bufs.find(nm + std::to_string(i));
+                if (it != c->bufs.end() && r1 < n) {
+                    cudaFree(it->second.p);
+                    c->bufs.erase(it);
+                }
+            }
+        }
+        r0 = r1;
+    }
+    tm.stop();
+    for (int i = 0; i < n; i++) {
+        outs[i].row = ps[i].ny;
+        outs[i].col = ps[i].nx;
+        outs[i].n_slices = in[i].S_max;
+        outs[i].interval_x = ps[i].lx / ps[i].nx;
+        outs[i].interval_y = ps[i].ly / ps[i].ny;
+        outs[i].total_intensity = 0.0;
+        if (lat) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev0, done[i]));
+            lat[i] = ms;
+        }
+    }
 }
 
 }  // namespace msb

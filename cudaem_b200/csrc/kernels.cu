@@ -22,6 +22,7 @@ namespace msb {
 static std::atomic<int64_t> g_launches{0};
 int64_t kernel_launches() { return g_launches.load(); }
 void reset_kernel_launches() { g_launches.store(0); }
+void add_kernel_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 static void check_launch(const char* what)
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
     float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
     float2* etab = tw + 2 * N;
     for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD)
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_ADJ)
         for (int i = threadIdx.x; i < kExpTab; i += blockDim.x) etab[i] = a.exptab[i];
     __syncthreads();
     float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
@@ -138,9 +139,9 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
 
     const size_t row_off = ((size_t)b * ny + r) * N;
     float2 v[E];
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD) {
-        const float* vr =
-            a.sV + (size_t)wi.conf_slot * a.sV_slot_stride + ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_ADJ) {
+        const float* vr = (wi.sV ? wi.sV : a.sV + (size_t)wi.conf_slot * a.sV_slot_stride) +
+                          ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
         if (OP == ROW_T_FWD) {
 #pragma unroll
             for (int j = 0; j < E; j++) v[j] = make_float2(1.0f, 0.0f);
@@ -150,12 +151,28 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
         }
         // pass 0: inverse row FFT as conj(FFT(conj(x))), then the transmission;
         // pass 1: forward row FFT.  One copy of the transform code serves both.
+        // ROW_ADJ is the adjoint of the same operator: with xbar the inverse row transform of the
+        // adjoint wave and x = t psi the stored forward wave, dL/dV += Re(i x conj(xbar)) and the
+        // adjoint continues as conj(t) xbar (or_stem_backward's chain, restated per row).
 #pragma unroll 1
         for (int pass = (OP == ROW_T_FWD) ? 1 : 0; pass < 2; pass++) {
             if (pass == 0) conj_all(v);
-            else if (!beyond) {
+            else if (OP == ROW_ADJ) {
+                const float2* xr = a.xs + row_off;
+                float* gr = a.dV + (size_t)r * N;
+#pragma unroll
+                for (int j = 0; j < E; j++) {
+                    const float2 x = __ldg(xr + g + G * j);
+                    atomicAdd(gr + g + G * j, x.x * v[j].y - x.y * v[j].x);
+                    v[j] = cmulc(v[j], expi_tab(__ldg(vr + g + G * j), etab));
+                }
+            } else if (!beyond) {
 #pragma unroll
                 for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + g + G * j), etab));
+                if (a.flags & PF_STORE_X) {
+#pragma unroll
+                    for (int j = 0; j < E; j++) a.xs[row_off + g + G * j] = v[j];
+                }
             }
             team_fft<N, G, -1>(v, g, tw, scr, sync);
             if (pass == 0) conj_all(v);
@@ -245,7 +262,7 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
 #pragma unroll
     for (int j = 0; j < E; j++) v[j] = cp[j * cs];
 
-    if (OP == COL_STEP || OP == COL_STEP_SEP) {
+    if constexpr (OP == COL_STEP || OP == COL_STEP_SEP) {
         // pass 0: forward column FFT, then P (or stop: the exit wave of the wave's last slice);
         // pass 1: inverse column FFT as conj(FFT(conj(x))).  One copy of the transform code.
 #pragma unroll 1
@@ -261,9 +278,14 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
                 // tabulated once per grid in FP64 and rounded to FP32; shared by every wave, so it stays in L2.
                 // The barrier keeps the table loads after the transform, so they do not hold registers
                 // across it.
-                const float2* pp = opaque(a.prop + (size_t)g * nx + col);
+                const float2* pp = opaque((wi.prop ? wi.prop : a.prop) + (size_t)g * nx + col);
+                if (a.flags & PF_CONJ_PROP) {
 #pragma unroll
-                for (int j = 0; j < E; j++) v[j] = cmul(v[j], __ldg(pp + j * cs));
+                    for (int j = 0; j < E; j++) v[j] = cmulc(v[j], __ldg(pp + j * cs));
+                } else {
+#pragma unroll
+                    for (int j = 0; j < E; j++) v[j] = cmul(v[j], __ldg(pp + j * cs));
+                }
             } else {
                 // P formed per element from the separable FP64-rounded phase factors and the band limit
                 // (where no table may be stored)
@@ -274,7 +296,8 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
                     float amp = a.grid.inv_n;
                     float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
                     if (a.grid.bwl) amp = amp / (1.0f + expf(a.grid.alpha_f * (g2 - a.grid.gl2_f)));
-                    v[j] = cmul(v[j], cscale(cmul(px, __ldg(a.prop_y + k)), amp));
+                    const float2 P = cscale(cmul(px, __ldg(a.prop_y + k)), amp);
+                    v[j] = (a.flags & PF_CONJ_PROP) ? cmulc(v[j], P) : cmul(v[j], P);
                 }
             }
             if (a.flags & PF_FILTER_AUX) {
@@ -289,7 +312,7 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
             }
             conj_all(v);
         }
-    } else if (OP == COL_CTF_INV) {
+    } else if constexpr (OP == COL_CTF_INV) {
         // apply_CTF_kernel (device_kernels.cuh:445-468)
         const double gx = freq_d(col, nx, a.grid.dgx);
 #pragma unroll
@@ -304,8 +327,66 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
             }
         }
         team_fft<N, G, +1>(v, g, tw, scr, sync);
-    } else if (OP == COL_INV) {
+    } else if constexpr (OP == COL_INV) {
         team_fft<N, G, +1>(v, g, tw, scr, sync);
+    } else if constexpr (OP == COL_SEED) {
+        // lambda(k) = sum_d 4 (I_d - T_d) Psi(k) [g^2 in annulus d], then the inverse column FFT
+        // (the first adjoint step of or_stem_backward: mu = D^H lambda, here its column half)
+        const double* rs = a.resid + (size_t)b * a.ndet;
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int k = g + G * j;
+            const float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+            double f = 0.0;
+            for (int d = 0; d < a.ndet; d++)
+                if (a.det_thr[d] <= g2 && g2 <= a.det_thr[a.ndet + d]) f += rs[d];
+            v[j] = cscale(v[j], (float)f);
+        }
+        team_fft<N, G, +1>(v, g, tw, scr, sync);
+    } else if constexpr (OP == COL_GRAD_PROBE) {
+        // Psi0bar = forward column FFT of the row-transformed adjoint; q = Re(i Psi0 conj(Psi0bar))
+        // with Psi0 regenerated exactly as COL_PROBE_INV does; sums of g^2 q and g^4 q give
+        // dL/dC10 and dL/dC30 (or_stem_backward's lens-phase gradient).
+        team_fft<N, G, -1>(v, g, tw, scr, sync);
+        const double gx = freq_d(col, nx, a.grid.dgx);
+        const double xf = -6.283185307179586476925 * wi.px, yf = -6.283185307179586476925 * wi.py;
+        double s2 = 0.0, s4 = 0.0;
+#pragma unroll
+        for (int j = 0; j < E; j++) {
+            const int k = g + G * j;
+            const float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+            if (a.lens.g2min <= g2 && g2 < a.lens.g2max) {
+                const double gy = freq_d(k, N, a.grid.dgy);
+                const float2 w0 = expi_d(chi_d(a.lens, wi.cc10, gx, gy) + xf * gx + yf * gy);
+                const double q = (double)w0.x * v[j].y - (double)w0.y * v[j].x;
+                const double gg = gx * gx + gy * gy;
+                s2 += gg * q;
+                s4 += gg * gg * q;
+            }
+        }
+        __shared__ double red[2][32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s2 += __shfl_down_sync(0xffffffffu, s2, o);
+            s4 += __shfl_down_sync(0xffffffffu, s4, o);
+        }
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) {
+            red[0][wid] = s2;
+            red[1][wid] = s4;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t2 = 0.0, t4 = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+                t2 += red[0][w];
+                t4 += red[1][w];
+            }
+            double* o = a.chi_part + ((size_t)b * tiles + (size_t)(col0 / TC)) * 2;
+            o[0] = t2;
+            o[1] = t4;
+        }
+        return;
     }
     cp = opaque(cp);
 #pragma unroll
@@ -336,6 +417,11 @@ static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStre
         cudaFuncSetAttribute(k_row<N, ROW_INV_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_row<N, ROW_INV_STORE><<<grid, block, sm, st>>>(a);
         break;
+    case ROW_ADJ:
+        cudaFuncSetAttribute(k_row<N, ROW_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row<N, ROW_ADJ><<<grid, block, sm, st>>>(a);
+        break;
+    default: throw MsError(MS_ERR_INTERNAL, "unknown row pass");
     }
 }
 
@@ -366,6 +452,15 @@ static void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStre
         cudaFuncSetAttribute(k_col<N, COL_STEP_SEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_col<N, COL_STEP_SEP><<<grid, block, sm, st>>>(a);
         break;
+    case COL_SEED:
+        cudaFuncSetAttribute(k_col<N, COL_SEED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_SEED><<<grid, block, sm, st>>>(a);
+        break;
+    case COL_GRAD_PROBE:
+        cudaFuncSetAttribute(k_col<N, COL_GRAD_PROBE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col<N, COL_GRAD_PROBE><<<grid, block, sm, st>>>(a);
+        break;
+    default: throw MsError(MS_ERR_INTERNAL, "unknown column pass");
     }
 }
 
@@ -421,6 +516,65 @@ void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream
     }
     count_launch();
     check_launch("column pass");
+}
+
+int col_tiles(int N, int nx)
+{
+    switch (N) {
+    case 128: return nx / FftLayout<128>::TC;
+    case 256: return nx / FftLayout<256>::TC;
+    case 512: return nx / FftLayout<512>::TC;
+    case 1024: return nx / FftLayout<1024>::TC;
+    case 2048: return nx / FftLayout<2048>::TC;
+    }
+    throw MsError(MS_ERR_UNSUPPORTED, "unsupported column length");
+}
+
+// Residuals of the detector loss: resid = 4 (I - target), sq = (I - target)^2.
+__global__ void k_resid(const double* I, const float* target, int n, double* resid, double* sq)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double r = I[i] - (double)target[i];
+    resid[i] = 4.0 * r;
+    sq[i] = r * r;
+}
+
+void launch_resid(const double* I, const float* target, int n, double* resid, double* sq, cudaStream_t st)
+{
+    k_resid<<<(n + 127) / 128, 128, 0, st>>>(I, target, n, resid, sq);
+    count_launch();
+    check_launch("loss residuals");
+}
+
+// Sums the lens-phase gradient partials of every wave in a fixed order into acc[0..1].
+__global__ void k_chi_finalize(const double* part, int n, double* acc)
+{
+    __shared__ double red[2][256];
+    double s2 = 0.0, s4 = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        s2 += part[2 * i];
+        s4 += part[2 * i + 1];
+    }
+    red[0][threadIdx.x] = s2;
+    red[1][threadIdx.x] = s4;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t2 = 0.0, t4 = 0.0;
+        for (int k = 0; k < (int)blockDim.x; k++) {
+            t2 += red[0][k];
+            t4 += red[1][k];
+        }
+        acc[0] += t2;
+        acc[1] += t4;
+    }
+}
+
+void launch_chi_finalize(const double* part, int nwaves, int nparts, double* acc, cudaStream_t st)
+{
+    k_chi_finalize<<<1, 256, 0, st>>>(part, nwaves * nparts, acc);
+    count_launch();
+    check_launch("lens gradient sum");
 }
 
 size_t row_smem(int N)

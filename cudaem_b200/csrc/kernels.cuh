@@ -9,12 +9,14 @@ namespace msb {
 
 // One wave of a batch.
 struct WaveInfo {
-    double px, py;   // probe position, Angstrom
-    double cc10;     // -pi (C10 + z_init) lambda of the probe, gated like Lens_Dev
-    int conf_slot;   // which potential slot (configuration) the wave reads
-    int n_slices;    // slices of the wave's specimen
-    float weight;    // configuration weight
-    int pos;         // output index (scan position) of the wave
+    double px = 0.0, py = 0.0;   // probe position, Angstrom
+    double cc10 = 0.0;           // -pi (C10 + z_init) lambda of the probe, gated like Lens_Dev
+    int conf_slot = 0;           // which potential slot (configuration) the wave reads
+    int n_slices = 0;            // slices of the wave's specimen
+    float weight = 1.0f;         // configuration weight
+    int pos = 0;                 // output index (scan position) of the wave
+    const float* sV = nullptr;      // if set: this wave's own potential store [slice][ny][nx] (uneven batches)
+    const float2* prop = nullptr;   // if set: this wave's own propagator table [ny][nx]
 };
 
 struct GridDev {
@@ -33,14 +35,24 @@ struct LensDev {
     float g2min, g2max;
 };
 
-enum RowOp { ROW_T_FWD = 0, ROW_INV_T_FWD = 1, ROW_INV_ABS2 = 2, ROW_INV_STORE = 3 };
-enum ColOp { COL_PROBE_INV = 0, COL_STEP = 1, COL_INV = 2, COL_CTF_INV = 3, COL_STEP_SEP = 4 };
+enum RowOp { ROW_T_FWD = 0, ROW_INV_T_FWD = 1, ROW_INV_ABS2 = 2, ROW_INV_STORE = 3, ROW_ADJ = 4 };
+enum ColOp {
+    COL_PROBE_INV = 0,
+    COL_STEP = 1,
+    COL_INV = 2,
+    COL_CTF_INV = 3,
+    COL_STEP_SEP = 4,
+    COL_SEED = 5,        // adjoint seed: annulus-weighted residuals times Psi, then inverse column FFT
+    COL_GRAD_PROBE = 6   // adjoint end: forward column FFT, then the lens-phase gradient sums
+};
 
 enum PassFlags {
     PF_VACUUM_BEYOND = 1,  // slices past a wave's own count are empty (t = 1) instead of skipped
     PF_ACCUMULATE = 2,     // ROW_INV_ABS2 adds into its output
     PF_FILTER_AUX = 4,     // COL_STEP also writes the annulus-filtered spectrum to aux
-    PF_PROP_ALWAYS = 8     // COL_STEP propagates even after the wave's last slice
+    PF_PROP_ALWAYS = 8,    // COL_STEP propagates even after the wave's last slice
+    PF_STORE_X = 16,       // ROW_INV_T_FWD also writes the transmitted real-space wave to xs
+    PF_CONJ_PROP = 32      // COL_STEP multiplies by conj(P) (the adjoint step)
 };
 
 struct PassArgs {
@@ -61,6 +73,13 @@ struct PassArgs {
     GridDev grid;
     LensDev lens;
     float filt_g2in, filt_g2out;
+    // adjoint
+    float2* xs;               // [B][ny][nx] transmitted real-space waves t_s psi_s of one slice
+    float* dV;                // [ny][nx] dL/dV of one slice, accumulated over waves
+    const double* resid;      // [B][ndet] 4 (I - target) per wave and detector
+    const float* det_thr;     // [2][ndet] inner, outer g^2 thresholds
+    int ndet;
+    double* chi_part;         // [B][nx / TC][2] partial sums of g^2 q and g^4 q
 };
 
 // Spatial cells of the atom binning: a ncx x ncy grid of square cells of side 1/inv_cell.
@@ -132,7 +151,13 @@ void launch_d2f(const double* in, int64_t n, float* out, cudaStream_t st);
 void launch_scan_counts(const unsigned* counts, int n, int64_t* seg, cudaStream_t st);
 void launch_fill_c(float2* p, int64_t n, float2 v, cudaStream_t st);
 
+// adjoint helpers
+void launch_resid(const double* I, const float* target, int n, double* resid, double* sq, cudaStream_t st);
+void launch_chi_finalize(const double* part, int nwaves, int nparts, double* acc, cudaStream_t st);
+int col_tiles(int N, int nx);
+
 int64_t kernel_launches();     // running count of this library's launches
 void reset_kernel_launches();
+void add_kernel_launches(int64_t n);   // launches replayed through (or captured into) a CUDA graph
 
 }  // namespace msb

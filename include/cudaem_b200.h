@@ -177,8 +177,16 @@ ms_status ms_set_stream(ms_ctx* ctx, void* cuda_stream);
 void* ms_get_stream(ms_ctx* ctx);
 /* Device time (ms) of the last simulate call, measured with CUDA events on the context stream. */
 double ms_last_device_ms(const ms_ctx* ctx);
-/* Number of this library's kernels launched by the last call. */
+/* Number of this library's kernels launched by the last call (kernels replayed from a
+ * captured CUDA graph included). */
 int64_t ms_last_launch_count(const ms_ctx* ctx);
+/* Probes per batch used by the last STEM call: the autotuner's choice when probe_batch is 0.
+ * No reference counterpart (the reference's batch is the fixed c_Probe_Batch,
+ * multislice_params_dev.cuh:92-108). */
+int ms_last_probe_batch(const ms_ctx* ctx);
+/* Enables (1, the default) or disables (0) replaying each STEM probe batch from a captured
+ * CUDA graph.  Disabled, every launch is issued directly; the results are identical. */
+ms_status ms_set_graphs(ms_ctx* ctx, int enable);
 
 /* Per-kernel timing (no reference counterpart: the reference has no tracing).  While enabled,
  * every fused pass and potential launch is bracketed by CUDA events on the context stream;
@@ -248,10 +256,14 @@ ms_status ms_stem_forward_potential(ms_ctx* ctx, const ms_params* p, const float
  * on the GPU race and must be serialised.  Errors are read with ms_last_error(NULL). */
 ms_status ms_stem_forward_potential_noalloc(void* cuda_stream, const ms_params* p, const float* V, int n_slices,
                                             double z_init, const double* probe_xy, int n_probe, float* I_out);
-/* Adjoint of ms_stem_forward_potential for the loss L = sum (I - target)^2:
+/* Adjoint of ms_stem_forward_potential for the loss L = sum_{probe,det} (I - target)^2:
  * loss, dL/dV [n_slices][ny][nx] (summed over probes) and dL/dC10, dL/dC30 of the condenser
- * lens.  Slices are checkpointed every p->ckpt_interval and recomputed.  No reference
- * counterpart: the reference has no differentiable path. */
+ * lens (C10 includes z_init; C30 is Cs).  The waves are checkpointed every p->ckpt_interval
+ * slices and each segment's transmitted waves are recomputed from its checkpoint.  V and
+ * dL_dV are device pointers when V_on_device is 1, host pointers otherwise; probe_xy and
+ * target ([n_probe][n_det]) are host memory.  dL/dV is summed over probes with atomic adds,
+ * so its last bits may differ between runs.  No reference counterpart: the reference has no
+ * differentiable path. */
 ms_status ms_stem_backward(ms_ctx* ctx, const ms_params* p, const float* V, int n_slices, int V_on_device,
                            double z_init, const double* probe_xy, int n_probe, const float* target,
                            double* loss, float* dL_dV, double* dL_dC10, double* dL_dC30);

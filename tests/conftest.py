@@ -14,9 +14,11 @@ def pytest_configure(config):
 
 
 def rel_l2(x, ref) -> float:
-    x = np.asarray(x, np.float64)
-    ref = np.asarray(ref, np.float64)
-    return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
+    x, ref = np.asarray(x), np.asarray(ref)
+    dt = np.complex128 if (np.iscomplexobj(x) or np.iscomplexobj(ref)) else np.float64
+    x = x.astype(dt)
+    ref = ref.astype(dt)
+    return float(np.linalg.norm((x - ref).ravel()) / np.linalg.norm(ref.ravel()))
 
 
 @pytest.fixture(scope="session")
