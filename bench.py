@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-vs-plain, adjoint and uneven-batch measurements")
+    ap.add_argument("--pass-kernels", type=int, default=0, choices=[0, 1],
+                    help="slice-pass kernel form: 0 classic (default), 1 persistent pipelined")
     ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
     ap.add_argument("--nconf", type=int, default=0, help="phonon configurations (0: the workload's)")
     return ap.parse_args()
@@ -241,9 +243,16 @@ def extras(ctx):
                                      C.byref(loss), gptr, C.byref(g10), C.byref(g30)))
         bw.append(ctx.last_device_ms)
     f, b = min(fw[1:]), min(bw[1:])
+    classes = ("row", "col", "probe", "row_store", "row_adj", "col_adj", "seed", "grad_probe")
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    ctx.check(L.ms_stem_backward(ctx.handle, C.byref(cp), vptr, V.shape[0], 1, z0, dptr, xy.shape[0], fptr(T),
+                                 C.byref(loss), gptr, C.byref(g10), C.byref(g30)))
+    split = {k: round(ctx.profile(k)[1], 3) for k in classes}
+    ctx.set_profiling(False)
     out["adjoint"] = {"workload": "differentiable STEM SrTiO3[001] 10x10x40 cells, 512^2, 80 slices, 200 kV, "
                                   "22 mrad, 16 probes, ADF loss, checkpoints every 8 slices",
-                      "forward_ms": f, "backward_ms": b, "ratio": b / f,
+                      "forward_ms": f, "backward_ms": b, "ratio": b / f, "backward_kernel_ms": split,
                       "note": "backward = loss, dL/dV, dL/dC10, dL/dC30 in one call (its own forward sweep included)"}
 
     # uneven batch: 64 CBED instances, 256^2..2048^2, 10-200 slices, 80-300 kV, 10-30 mrad
@@ -309,6 +318,7 @@ def run_ours(args):
     if args.cells_z or args.nconf:
         desc = dict(desc, workload=desc["workload"] + f" [reduced: cells_z={args.cells_z}, nconf={args.nconf}]")
     ctx = cb.Context(local)
+    ctx.set_pass_kernels(args.pass_kernels)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     L = cb.lib()

@@ -262,6 +262,10 @@ class Context:
     def set_graphs(self, enable: bool) -> None:
         self.check(lib().ms_set_graphs(self.handle, 1 if enable else 0))
 
+    def set_pass_kernels(self, variant: int) -> None:
+        """0: classic one-block-per-tile slice passes (default); 1: persistent pipelined passes."""
+        self.check(lib().ms_set_pass_kernels(self.handle, variant))
+
     def set_profiling(self, enable: bool) -> None:
         self.check(lib().ms_set_profiling(self.handle, 1 if enable else 0))
 

@@ -160,6 +160,18 @@ int64_t ms_last_launch_count(const ms_ctx* c) { return c ? c->last_launches : 0;
 
 int ms_last_probe_batch(const ms_ctx* c) { return c ? c->last_batch : 0; }
 
+ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
+{
+    if (!c || (variant != 0 && variant != 1)) return MS_ERR_INVALID_ARG;
+    c->pass_variant = variant;
+    if (c->stream) {
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+    }
+    c->drop_graph();   // captured graphs hold the other kernels
+    return MS_OK;
+}
+
 ms_status ms_set_graphs(ms_ctx* c, int enable)
 {
     if (!c) return MS_ERR_INVALID_ARG;

@@ -36,6 +36,7 @@ struct ms_ctx {
     };
     std::map<std::string, Graph> graphs;         // keyed by the launch arguments they bake in
     bool use_graphs = true;
+    int pass_variant = 0;                        // msb::PassVariant of the slice-pass kernels (0: classic)
     int last_batch = 0;                          // probe batch used by the last STEM call
     std::vector<cudaStream_t> side;              // streams of the grid groups of an uneven batch
     std::map<std::string, int> batch_choice;     // autotuned probe batch per grid and slice count

@@ -119,14 +119,22 @@ void timed(ms_ctx* c, const char* cls, F&& launch)
     c->ev_pending.emplace_back(cls, i0);
 }
 
+// Kernel classes of the per-launch timing: the forward passes are "row" and "col"; the
+// adjoint's own launches get classes of their own.
 void run_row(ms_ctx* c, int N, int op, const PassArgs& a, int nw, int ny, cudaStream_t st)
 {
-    timed(c, "row", [&] { launch_row(N, op, a, nw, ny, st); });
+    const char* cls = op == ROW_ADJ ? "row_adj" : ((a.flags & PF_STORE_X) ? "row_store" : "row");
+    timed(c, cls, [&] { launch_row(N, op, a, nw, ny, st); });
 }
 
 void run_col(ms_ctx* c, int N, int op, const PassArgs& a, int nw, int nx, cudaStream_t st)
 {
-    timed(c, op == COL_PROBE_INV ? "probe" : "col", [&] { launch_col(N, op, a, nw, nx, st); });
+    const char* cls = op == COL_PROBE_INV       ? "probe"
+                      : op == COL_SEED          ? "seed"
+                      : op == COL_GRAD_PROBE    ? "grad_probe"
+                      : (a.flags & PF_CONJ_PROP) ? "col_adj"
+                                                 : "col";
+    timed(c, cls, [&] { launch_col(N, op, a, nw, nx, st); });
 }
 
 void run_potential(ms_ctx* c, const PotArgs& a, int n_conf, cudaStream_t st)
@@ -198,11 +206,13 @@ struct Setup {
     const float2* prop;
     const float2* exptab;
     int64_t N;
+    int variant = PASS_CLASSIC;
 };
 
 Setup make_setup(ms_ctx* c, const ms_params& p)
 {
     Setup s;
+    s.variant = c->pass_variant;
     s.ph = physics_of(p.E0, p.theta);
     s.gc = grid_of(p, s.ph);
     s.N = (int64_t)p.nx * p.ny;
@@ -491,6 +501,7 @@ PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const flo
     a.exptab = s.exptab;
     a.grid = s.gd;
     a.lens = lens;
+    a.variant = s.variant;
     return a;
 }
 

@@ -41,6 +41,7 @@ struct FftLayout {
     static constexpr int ROW_THREADS = ROWS * G;
     static constexpr int COL_THREADS = TC * G;
     static constexpr int COL_MINB = (N == 2048) ? 1 : 2;   // resident column blocks per SM (register cap)
+    static constexpr int ROW_MINB = (N == 2048) ? 1 : 2;   // resident row blocks per SM (register cap)
     // transpose scratch of one transform: E rows of G+1 slots, plus padding so that
     // consecutive transforms start on banks that keep a half-warp conflict-free
     static constexpr int SCR_BASE = E * (G + 1);

@@ -10,6 +10,7 @@
 // HRTEM column pass and the detector sums in a read-only post pass.
 #include <cub/device/device_radix_sort.cuh>
 
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 
@@ -113,7 +114,7 @@ __device__ __forceinline__ void conj_all(float2 (&v)[E])
 // row pass
 // ---------------------------------------------------------------------------
 template <int N, int OP>
-__global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
+__global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_MINB) k_row(PassArgs a)
 {
     using L = FftLayout<N>;
     constexpr int G = L::G, E = L::E;
@@ -125,29 +126,32 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
     const int r = (blockIdx.x % blocks_per_wave) * L::ROWS + team;
     const WaveInfo wi = a.waves[b];
     const bool beyond = a.slice >= wi.n_slices;
-    if ((OP == ROW_T_FWD || OP == ROW_INV_T_FWD) && beyond && !(a.flags & PF_VACUUM_BEYOND)) return;
+    if ((OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X) && beyond && !(a.flags & PF_VACUUM_BEYOND))
+        return;
 
+    const size_t row_off = ((size_t)b * ny + r) * N;
+    float2 v[E];
+    // the wave's loads go out first, so their latency overlaps the table staging below
+    if (OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_ADJ) {
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = a.psi[row_off + g + G * j];
+    }
     float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
     float2* etab = tw + 2 * N;
     for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_ADJ)
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_ADJ)
         for (int i = threadIdx.x; i < kExpTab; i += blockDim.x) etab[i] = a.exptab[i];
     __syncthreads();
     float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
     auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
     auto sync = []() { __syncwarp(); };
 
-    const size_t row_off = ((size_t)b * ny + r) * N;
-    float2 v[E];
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_ADJ) {
+    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_ADJ) {
         const float* vr = (wi.sV ? wi.sV : a.sV + (size_t)wi.conf_slot * a.sV_slot_stride) +
                           ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
         if (OP == ROW_T_FWD) {
 #pragma unroll
             for (int j = 0; j < E; j++) v[j] = make_float2(1.0f, 0.0f);
-        } else {
-#pragma unroll
-            for (int j = 0; j < E; j++) v[j] = a.psi[row_off + g + G * j];
         }
         // pass 0: inverse row FFT as conj(FFT(conj(x))), then the transmission;
         // pass 1: forward row FFT.  One copy of the transform code serves both.
@@ -169,7 +173,7 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS) k_row(PassArgs a)
             } else if (!beyond) {
 #pragma unroll
                 for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + g + G * j), etab));
-                if (a.flags & PF_STORE_X) {
+                if constexpr (OP == ROW_INV_T_FWD_X) {
 #pragma unroll
                     for (int j = 0; j < E; j++) a.xs[row_off + g + G * j] = v[j];
                 }
@@ -223,13 +227,6 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
         final_step = (a.slice == wi.n_slices - 1) && !(a.flags & PF_PROP_ALWAYS);
     }
 
-    float2* tw = smem + TC * L::SCR_STRIDE_COL;
-    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
-    __syncthreads();
-    float2* scr_base = smem + c * L::SCR_STRIDE_COL;
-    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
-    auto sync = []() { __syncthreads(); };
-
     float2* base = a.psi + (size_t)b * N * nx;
     // element (g + G j, col) of the wave sits at cp[j * cs]; the pointer is made opaque before each
     // later use so the compiler recomputes the E addresses (one IMAD each) instead of keeping E
@@ -237,6 +234,17 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
     float2* cp = base + (size_t)g * nx + col;
     const size_t cs = (size_t)G * nx;
     float2 v[E];
+    // the wave's loads go out first, so their latency overlaps the table staging below
+    if constexpr (OP != COL_PROBE_INV) {
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = cp[j * cs];
+    }
+    float2* tw = smem + TC * L::SCR_STRIDE_COL;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
+    __syncthreads();
+    float2* scr_base = smem + c * L::SCR_STRIDE_COL;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncthreads(); };
     if constexpr (OP == COL_PROBE_INV) {
         // Generate_probe / Generate_multi_probe (device_kernels.cuh:363-444): aperture mask on the
         // float frequency, phase chi + x gx + y gy formed in FP64.
@@ -259,9 +267,6 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
         for (int j = 0; j < E; j++) cp[j * cs] = v[j];
         return;
     } else {
-#pragma unroll
-    for (int j = 0; j < E; j++) v[j] = cp[j * cs];
-
     if constexpr (OP == COL_STEP || OP == COL_STEP_SEP) {
         // pass 0: forward column FFT, then P (or stop: the exit wave of the wave's last slice);
         // pass 1: inverse column FFT as conj(FFT(conj(x))).  One copy of the transform code.
@@ -394,12 +399,284 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
     }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent, software-pipelined forms of the two slice passes (ROW_INV_T_FWD and
+// COL_STEP with the propagator table).  One block of 256 threads per SM stays resident
+// and walks the pass's work items with a grid stride; the twiddle and exp tables are
+// staged into shared memory once per block instead of once per item.  While an item is
+// transformed, the next item's wave values are already in flight into registers (the
+// block has the whole register file: 255 per thread), the row pass issues the item's
+// potential loads before its first transform, and the column pass brings the next item's
+// propagator tile into shared memory with cp.async.  The arithmetic is the classic
+// kernels' (the compiler may contract a few products differently, so the two forms agree
+// to about one rounding per operation rather than bit for bit).
+// ---------------------------------------------------------------------------
+constexpr int kPipeThreads = 256;
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <int N>
+__global__ void __launch_bounds__(kPipeThreads, 1) k_row_p(PassArgs a, int nwaves)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E;
+    constexpr int R = 32 / G;                       // rows per warp item (one per team)
+    constexpr int WARPS = kPipeThreads / 32;
+    constexpr int VROW = R * N;                     // potential floats of one item
+    // cp.async destinations must sit on 16-byte boundaries
+    static_assert(((WARPS * R * L::SCR_STRIDE_ROW + 2 * N + kExpTab) * sizeof(float2)) % 16 == 0, "vbuf alignment");
+    static_assert((VROW * sizeof(float)) % 16 == 0, "vbuf alignment");
+    extern __shared__ float2 smem[];
+    float2* tw = smem + WARPS * R * L::SCR_STRIDE_ROW;
+    float2* etab = tw + 2 * N;
+    float* vbuf_all = reinterpret_cast<float*>(etab + kExpTab);   // [WARPS][2][VROW]
+    for (int i = threadIdx.x; i < 2 * N; i += kPipeThreads) tw[i] = a.tw[i];
+    for (int i = threadIdx.x; i < kExpTab; i += kPipeThreads) etab[i] = a.exptab[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tm = lane / G, g = lane % G;
+    float2* scr_base = smem + (warp * R + tm) * L::SCR_STRIDE_ROW;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncwarp(); };
+    float* vbuf = vbuf_all + warp * 2 * VROW;
+    const int ny = a.grid.ny;
+    const int64_t n_items = (int64_t)nwaves * ny / R;
+    const int64_t stride = (int64_t)gridDim.x * WARPS;
+    const bool vac = (a.flags & PF_VACUUM_BEYOND) != 0;
+    // items whose wave has no slice here are skipped whole (the classic kernel's early return)
+    auto next_live = [&](int64_t it) {
+        while (it < n_items && !vac && a.slice >= a.waves[(int)((it * R) / ny)].n_slices) it += stride;
+        return it;
+    };
+    // the item's R potential rows (contiguous: the rows of one wave) into vbuf[buf], 16 bytes a piece
+    auto fetch_pot = [&](int64_t it, int buf) {
+        const int64_t row0 = it * R;
+        const int b = (int)(row0 / ny), r0 = (int)(row0 % ny);
+        const WaveInfo& wi = a.waves[b];
+        if (a.slice < wi.n_slices) {
+            const float* vr = (wi.sV ? wi.sV : a.sV + (size_t)wi.conf_slot * a.sV_slot_stride) +
+                              ((size_t)(a.slice - a.sV_slice_base) * ny + r0) * N;
+            for (int q = lane; q < VROW / 4; q += 32) cp_async16(vbuf + buf * VROW + 4 * q, vr + 4 * q);
+        }
+        cp_async_commit();
+    };
+    int64_t it = next_live((int64_t)blockIdx.x * WARPS + warp);
+    float2 vn[E];
+    if (it < n_items) {
+        const float2* src = a.psi + (it * R + tm) * N;
+#pragma unroll
+        for (int j = 0; j < E; j++) vn[j] = src[g + G * j];
+        fetch_pot(it, 0);
+    }
+    int buf = 0;
+    while (it < n_items) {
+        const int64_t row = it * R + tm;
+        const int b = (int)(row / ny);
+        float2 v[E];
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = vn[j];
+        const int64_t nxt = next_live(it + stride);
+        if (nxt < n_items) {
+            const float2* src = a.psi + (nxt * R + tm) * N;
+#pragma unroll
+            for (int j = 0; j < E; j++) vn[j] = src[g + G * j];
+            fetch_pot(nxt, buf ^ 1);
+        } else {
+            cp_async_commit();
+        }
+        const bool beyond = a.slice >= a.waves[b].n_slices;
+        const float* vv = vbuf + buf * VROW + tm * N;
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {
+            if (pass == 0) conj_all(v);
+            else if (!beyond) {
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(vv[g + G * j], etab));
+            }
+            team_fft<N, G, -1>(v, g, tw, scr, sync);
+            if (pass == 0) conj_all(v);
+        }
+        float2* dst = a.psi + row * N;
+#pragma unroll
+        for (int j = 0; j < E; j++) dst[g + G * j] = v[j];
+        buf ^= 1;
+        it = nxt;
+    }
+    cp_async_wait_all();
+}
+
+template <int N>
+__global__ void __launch_bounds__(kPipeThreads, 1) k_col_p(PassArgs a, int nwaves)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E, TC = L::TC;
+    static_assert(TC * G == kPipeThreads, "the column tile must occupy the whole block");
+    extern __shared__ float2 smem[];
+    float2* tw = smem + TC * L::SCR_STRIDE_COL;
+    float2* ptile = tw + 2 * N;                     // propagator tile [N][TC]
+    static_assert(((TC * L::SCR_STRIDE_COL + 2 * N) * sizeof(float2)) % 16 == 0, "ptile alignment");
+    static_assert(TC % 2 == 0, "16-byte propagator pieces");
+    for (int i = threadIdx.x; i < 2 * N; i += kPipeThreads) tw[i] = a.tw[i];
+    const int nx = a.grid.nx;
+    const int tiles = nx / TC;
+    const int64_t n_items = (int64_t)nwaves * tiles;
+    const bool vac = (a.flags & PF_VACUUM_BEYOND) != 0;
+    auto next_live = [&](int64_t it) {
+        while (it < n_items && !vac && a.slice >= a.waves[(int)(it / tiles)].n_slices) it += gridDim.x;
+        return it;
+    };
+    const int tid = threadIdx.x;
+    const int c = tid % TC, g = tid / TC;
+    float2* scr_base = smem + c * L::SCR_STRIDE_COL;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncthreads(); };
+    const size_t cs = (size_t)G * nx;
+    // the propagator tile of item `it`: N rows of TC float2, in 16-byte pieces
+    auto fetch_prop = [&](int64_t it) {
+        const int col0 = (int)(it % tiles) * TC;
+        const float2* P = (a.waves[(int)(it / tiles)].prop ? a.waves[(int)(it / tiles)].prop : a.prop) + col0;
+        constexpr int PIECES = N * TC / 2;
+        for (int q = tid; q < PIECES; q += kPipeThreads) {
+            const int row = q / (TC / 2), part = q % (TC / 2);
+            cp_async16(ptile + row * TC + 2 * part, P + (size_t)row * nx + 2 * part);
+        }
+        cp_async_commit();
+    };
+    int64_t it = next_live(blockIdx.x);
+    float2 vn[E];
+    if (it < n_items) {
+        const float2* cp = a.psi + (size_t)(it / tiles) * N * nx + (size_t)g * nx + (it % tiles) * TC + c;
+#pragma unroll
+        for (int j = 0; j < E; j++) vn[j] = cp[j * cs];
+        fetch_prop(it);
+    }
+    __syncthreads();
+    while (it < n_items) {
+        const int b = (int)(it / tiles);
+        const int col = (int)(it % tiles) * TC + c;
+        float2 v[E];
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = vn[j];
+        const int64_t nxt = next_live(it + gridDim.x);
+        if (nxt < n_items) {
+            const float2* cp = a.psi + (size_t)(nxt / tiles) * N * nx + (size_t)g * nx + (nxt % tiles) * TC + c;
+#pragma unroll
+            for (int j = 0; j < E; j++) vn[j] = cp[j * cs];
+        }
+        const WaveInfo& wi = a.waves[b];
+        const bool final_step = (a.slice == wi.n_slices - 1) && !(a.flags & PF_PROP_ALWAYS);
+        // forward column FFT, then P (or stop: the exit wave of the wave's last slice), then the
+        // inverse column FFT as conj(FFT(conj(x)))
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {
+            team_fft<N, G, -1>(v, g, tw, scr, sync);
+            if (pass == 1) {
+                conj_all(v);
+                break;
+            }
+            if (final_step) break;
+            cp_async_wait_all();
+            __syncthreads();
+            const float2* pp = ptile + g * TC + c;
+            if (a.flags & PF_CONJ_PROP) {
+#pragma unroll
+                for (int j = 0; j < E; j++) v[j] = cmulc(v[j], pp[j * G * TC]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < E; j++) v[j] = cmul(v[j], pp[j * G * TC]);
+            }
+            conj_all(v);
+        }
+        // every thread is past its reads of the tile: bring in the next item's
+        cp_async_wait_all();
+        __syncthreads();
+        if (nxt < n_items) fetch_prop(nxt);
+        float2* cp = a.psi + (size_t)b * N * nx + (size_t)g * nx + col;
+#pragma unroll
+        for (int j = 0; j < E; j++) cp[j * cs] = v[j];
+        it = nxt;
+    }
+    cp_async_wait_all();
+}
+
+// Grids of 128..1024 points for the row pass; the column pass needs a full 256-thread tile
+// (TC x G = 256: 256..1024 points).  2048-point passes use the classic kernels.
+template <int N>
+struct PipeSupported {
+    static constexpr bool value = (N >= 128 && N <= 1024);
+};
+template <int N>
+struct ColPipeSupported {
+    static constexpr bool value = (N >= 256 && N <= 1024 && FftLayout<N>::TC * FftLayout<N>::G == kPipeThreads);
+};
+
+int num_sms()
+{
+    static int n[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!n[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        n[dev] = v > 0 ? v : 148;
+    }
+    return n[dev];
+}
+
+template <int N>
+static bool row_pipe(const PassArgs& a, int nwaves, int ny, cudaStream_t st)
+{
+    if constexpr (!PipeSupported<N>::value) {
+        return false;
+    } else {
+        using L = FftLayout<N>;
+        constexpr int R = 32 / L::G;
+        const int64_t items = (int64_t)nwaves * ny / R;
+        const int64_t blocks = std::min<int64_t>((items + 7) / 8, num_sms());
+        const size_t sm = sizeof(float2) * ((size_t)(kPipeThreads / 32) * R * L::SCR_STRIDE_ROW + 2 * N + kExpTab) +
+                          sizeof(float) * (size_t)(kPipeThreads / 32) * 2 * R * N;
+        cudaFuncSetAttribute(k_row_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row_p<N><<<(unsigned)blocks, kPipeThreads, sm, st>>>(a, nwaves);
+        return true;
+    }
+}
+
+template <int N>
+static bool col_pipe(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
+{
+    if constexpr (!ColPipeSupported<N>::value) {
+        return false;
+    } else {
+        using L = FftLayout<N>;
+        const int64_t items = (int64_t)nwaves * (nx / L::TC);
+        const int64_t blocks = std::min<int64_t>(items, num_sms());
+        const size_t sm = sizeof(float2) * ((size_t)L::TC * L::SCR_STRIDE_COL + 2 * N + (size_t)N * L::TC);
+        cudaFuncSetAttribute(k_col_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_col_p<N><<<(unsigned)blocks, kPipeThreads, sm, st>>>(a, nwaves);
+        return true;
+    }
+}
+
 template <int N>
 static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st)
 {
     using L = FftLayout<N>;
+    // the pipelined form copies potential rows with 16-byte cp.async: it needs an aligned store
+    if (op == ROW_INV_T_FWD && a.variant == PASS_PIPELINED && !(a.flags & PF_STORE_X) &&
+        ((uintptr_t)a.sV & 15) == 0 && row_pipe<N>(a, nwaves, ny, st))
+        return;
     dim3 grid((unsigned)(nwaves * (ny / L::ROWS))), block(L::ROW_THREADS);
     size_t sm = L::ROW_SMEM;
+    if (op == ROW_INV_T_FWD && (a.flags & PF_STORE_X)) op = ROW_INV_T_FWD_X;
     switch (op) {
     case ROW_T_FWD:
         cudaFuncSetAttribute(k_row<N, ROW_T_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -421,6 +698,10 @@ static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStre
         cudaFuncSetAttribute(k_row<N, ROW_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_row<N, ROW_ADJ><<<grid, block, sm, st>>>(a);
         break;
+    case ROW_INV_T_FWD_X:
+        cudaFuncSetAttribute(k_row<N, ROW_INV_T_FWD_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_row<N, ROW_INV_T_FWD_X><<<grid, block, sm, st>>>(a);
+        break;
     default: throw MsError(MS_ERR_INTERNAL, "unknown row pass");
     }
 }
@@ -429,6 +710,9 @@ template <int N>
 static void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st)
 {
     using L = FftLayout<N>;
+    if (op == COL_STEP && a.variant == PASS_PIPELINED && !(a.flags & PF_FILTER_AUX) && ((uintptr_t)a.prop & 15) == 0 &&
+        col_pipe<N>(a, nwaves, nx, st))
+        return;
     dim3 grid((unsigned)(nwaves * (nx / L::TC))), block(L::COL_THREADS);
     size_t sm = L::COL_SMEM;
     switch (op) {
@@ -662,6 +946,10 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
         }
         const float X0 = (float)tx0 * a.dx, X1 = (float)(tx0 + kPotTX - 1) * a.dx;
         const float Y0 = (float)ty0 * a.dy, Y1 = (float)(ty0 + kPotTY - 1) * a.dy;
+        // this warp's block: pixels tx0 + [16 (wblk % 4), +16), ty0 + [16 (wblk / 4), +16), with a
+        // margin of one pixel for the float rounding of the block corners
+        const float WX0 = (float)(tx0 + (wblk % 4) * 16 - 1) * a.dx, WX1 = (float)(tx0 + (wblk % 4) * 16 + 16) * a.dx;
+        const float WY0 = (float)(ty0 + (wblk / 4) * 16 - 1) * a.dy, WY1 = (float)(ty0 + (wblk / 4) * 16 + 16) * a.dy;
         if (t == 0) {
             // Atoms are sorted by (configuration, slice, cell) with cells of a.cell A in a
             // ncx x ncy grid over the box.  The tile needs the cells its rectangle, grown by the
@@ -754,10 +1042,18 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
                 const int bits = __float_as_int(cd.w);
                 const ElemTable& T = el[bits & 0xFF];
                 const float rmax2 = T.rmax2;
+                const int ox = ((bits >> 8) & 15) - 4, oy = ((bits >> 12) & 15) - 4;
+                // warp-uniform skip: the atom's disc misses this warp's 16 x 16 pixel block (its
+                // spline evaluations would all be masked off, yet a divergent warp still issues them)
+                {
+                    const float xs = cd.x + (float)ox * a.lx, ys = cd.y + (float)oy * a.ly;
+                    const float dxr = fmaxf(0.f, fmaxf(WX0 - xs, xs - WX1));
+                    const float dyr = fmaxf(0.f, fmaxf(WY0 - ys, ys - WY1));
+                    if (dxr * dxr + dyr * dyr >= rmax2 * 1.0002f + 1e-4f) continue;
+                }
                 // distance to the image (ox, oy) of the atom: pixel index shifted by -ox*nx, and
                 // i*dx - x formed with dx split in two floats, so the offset is accurate to its own
                 // rounding (the pixel coordinate i*dx alone would carry ~1e-6 A of error)
-                const int ox = ((bits >> 8) & 15) - 4, oy = ((bits >> 12) & 15) - 4;
                 const float fx0 = (float)(tx0 + 4 * px - ox * a.nx), fy0 = (float)(ty0 + py - oy * a.ny);
                 float dx2[4], dy2[RY];
 #pragma unroll

@@ -35,7 +35,14 @@ struct LensDev {
     float g2min, g2max;
 };
 
-enum RowOp { ROW_T_FWD = 0, ROW_INV_T_FWD = 1, ROW_INV_ABS2 = 2, ROW_INV_STORE = 3, ROW_ADJ = 4 };
+enum RowOp {
+    ROW_T_FWD = 0,
+    ROW_INV_T_FWD = 1,
+    ROW_INV_ABS2 = 2,
+    ROW_INV_STORE = 3,
+    ROW_ADJ = 4,
+    ROW_INV_T_FWD_X = 5   // ROW_INV_T_FWD that also keeps t psi in xs (selected by PF_STORE_X)
+};
 enum ColOp {
     COL_PROBE_INV = 0,
     COL_STEP = 1,
@@ -80,7 +87,13 @@ struct PassArgs {
     const float* det_thr;     // [2][ndet] inner, outer g^2 thresholds
     int ndet;
     double* chi_part;         // [B][nx / TC][2] partial sums of g^2 q and g^4 q
+    int variant;              // PassVariant of the row / column pass kernels (host side only)
 };
+
+// Kernel form of ROW_INV_T_FWD and COL_STEP: the classic one-block-per-tile kernels (two
+// resident blocks per SM, the default: measured faster on B200 at 1024^2) or the persistent
+// pipelined kernels (grids of 128..1024 points).  Both compute the same operations.
+enum PassVariant { PASS_CLASSIC = 0, PASS_PIPELINED = 1 };
 
 // Spatial cells of the atom binning: a ncx x ncy grid of square cells of side 1/inv_cell.
 struct CellGrid {

@@ -187,11 +187,20 @@ int ms_last_probe_batch(const ms_ctx* ctx);
 /* Enables (1, the default) or disables (0) replaying each STEM probe batch from a captured
  * CUDA graph.  Disabled, every launch is issued directly; the results are identical. */
 ms_status ms_set_graphs(ms_ctx* ctx, int enable);
+/* Kernel form of the hot slice passes: 0 (default) the classic kernels, one block per tile
+ * of rows or columns with two blocks resident per SM; 1 the persistent pipelined kernels
+ * (one block per SM walking the work items, the next item's wave prefetched while the
+ * current one is transformed) for grids of 128..1024 points per axis.  Both compute the same
+ * operations (results agree to float rounding); the choice only changes speed.  No
+ * reference counterpart (the reference's passes are cuFFT plans). */
+ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
 
 /* Per-kernel timing (no reference counterpart: the reference has no tracing).  While enabled,
  * every fused pass and potential launch is bracketed by CUDA events on the context stream;
  * ms_profile_get returns the launches and summed device time of one kernel class
- * ("row", "col", "potential", "probe", "post") since the last reset. */
+ * since the last reset: "row", "col" (forward slice passes), "potential", "probe", and the
+ * adjoint's "row_store" (forward row pass that keeps the transmitted wave), "row_adj",
+ * "col_adj", "seed", "grad_probe". */
 ms_status ms_set_profiling(ms_ctx* ctx, int enable);
 ms_status ms_profile_reset(ms_ctx* ctx);
 ms_status ms_profile_get(const ms_ctx* ctx, const char* kernel, int64_t* launches, double* total_ms);
