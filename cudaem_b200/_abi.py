@@ -25,6 +25,7 @@ MS_IW_PLANE, MS_IW_CONVERGENT = 1, 2
 (MS_POT_DOYLE_0_4, MS_POT_PENG_0_4, MS_POT_PENG_0_12, MS_POT_KIRKLAND_0_12, MS_POT_WEICKENMEIER_0_12,
  MS_POT_LOBATO_0_12, MS_POT_MOLIERE) = range(1, 8)
 MS_ILLUM_COHERENT, MS_ILLUM_PARTIAL, MS_ILLUM_TCC = 1, 2, 3
+MS_TSI_TEMPORAL_SPATIAL, MS_TSI_TEMPORAL, MS_TSI_SPATIAL, MS_TSI_COHERENT = 1, 2, 3, 4
 MS_RECORD_INTENSITY, MS_RECORD_WAVE = 0, 1
 MS_EXEC_BATCHED, MS_EXEC_PLAIN = 0, 1
 MS_BORDER_MIN, MS_BORDER_MAX, MS_BORDER_MIDDLE = 0, 1, 2
@@ -36,7 +37,8 @@ class ms_lens(C.Structure):
         "c30", "c32", "phi32", "c34", "phi34",
         "c41", "phi41", "c43", "phi43", "c45", "phi45",
         "c50", "c52", "phi52", "c54", "phi54", "c56", "phi56",
-        "inner_aper_ang", "outer_aper_ang")]
+        "inner_aper_ang", "outer_aper_ang", "dsf_sigma", "ssf_beta")] + [
+        ("dsf_npoints", C.c_int), ("ssf_npoints", C.c_int)]
 
 
 class ms_element_coef(C.Structure):
@@ -74,6 +76,7 @@ class ms_params(C.Structure):
         ("cond_lens", ms_lens),
         ("obj_lens", ms_lens),
         ("illumination_model", C.c_int),
+        ("temporal_spatial_incoh", C.c_int),
         ("data_record", C.c_int),
         ("scan_nx", C.c_int), ("scan_ny", C.c_int),
         ("scan_x0", C.c_double), ("scan_y0", C.c_double),

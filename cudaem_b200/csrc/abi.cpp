@@ -61,6 +61,9 @@ void ms_default_params(ms_params* p)
     p->slice_border = -1;
     p->iw_type = -1;
     p->illumination_model = MS_ILLUM_COHERENT;
+    p->temporal_spatial_incoh = MS_TSI_TEMPORAL_SPATIAL;
+    p->obj_lens.dsf_npoints = p->cond_lens.dsf_npoints = 8;
+    p->obj_lens.ssf_npoints = p->cond_lens.ssf_npoints = 4;
     p->data_record = MS_RECORD_INTENSITY;
     p->thick_det = 0;
     p->exec_mode = MS_EXEC_BATCHED;

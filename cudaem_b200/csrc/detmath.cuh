@@ -189,4 +189,12 @@ MS_HD float det_g2(int ix, int iy, int nx, int ny, float dgx, float dgy)
     return MSF_ADD(MSF_MUL(gx, gx), MSF_MUL(gy, gy));
 }
 
+// The same with the frequencies shifted by (gxu, gyu) (apply_CTF_kernel's source-point shift,
+// device_kernels.cuh:454-456); a zero shift gives det_g2's value exactly.
+MS_HD float det_g2_shift(int ix, int iy, int nx, int ny, float dgx, float dgy, float gxu, float gyu)
+{
+    float gx = MSF_ADD(det_gfreq(ix, nx, dgx), gxu), gy = MSF_ADD(det_gfreq(iy, ny, dgy), gyu);
+    return MSF_ADD(MSF_MUL(gx, gx), MSF_MUL(gy, gy));
+}
+
 }  // namespace msb

@@ -192,7 +192,64 @@ LensDev lens_dev(const LensCoef& L)
     d.p45 = L.p45; d.p52 = L.p52; d.p54 = L.p54; d.p56 = L.p56;
     d.g2min = L.g2min;
     d.g2max = L.g2max;
+    d.amp = 1.0;
     return d;
+}
+
+// Gauss-Hermite nodes and weights for exp(-x^2), weights normalised to sum 1: the Newton
+// iteration on the orthonormal Hermite recurrence with the usual asymptotic starting points
+// (the reference's quadrature tables come from the missing multislice_params.hpp).
+void gauss_hermite(int n, std::vector<double>* x, std::vector<double>* w)
+{
+    x->assign(n, 0.0);
+    w->assign(n, 1.0);
+    if (n == 1) return;
+    const double pim4 = 0.7511255444649425;
+    double z = 0.0, pp = 0.0;
+    const int m = (n + 1) / 2;
+    for (int i = 0; i < m; i++) {
+        if (i == 0) z = std::sqrt(2.0 * n + 1.0) - 1.85575 * std::pow(2.0 * n + 1.0, -0.16667);
+        else if (i == 1) z -= 1.14 * std::pow((double)n, 0.426) / z;
+        else if (i == 2) z = 1.86 * z - 0.86 * (*x)[0];
+        else if (i == 3) z = 1.91 * z - 0.91 * (*x)[1];
+        else z = 2.0 * z - (*x)[i - 2];
+        for (int it = 0; it < 100; it++) {
+            double p1 = pim4, p2 = 0.0;
+            for (int j = 1; j <= n; j++) {
+                const double p3 = p2;
+                p2 = p1;
+                p1 = z * std::sqrt(2.0 / j) * p2 - std::sqrt((double)(j - 1) / j) * p3;
+            }
+            pp = std::sqrt(2.0 * n) * p2;
+            const double z1 = z;
+            z = z1 - p1 / pp;
+            if (std::fabs(z - z1) <= 1e-15 * (1.0 + std::fabs(z))) break;
+        }
+        (*x)[i] = z;
+        (*x)[n - 1 - i] = -z;
+        (*w)[i] = (*w)[n - 1 - i] = 2.0 / (pp * pp);
+    }
+    if (n % 2 == 1) (*x)[m - 1] = 0.0;
+    double sw = 0.0;
+    for (double v : *w) sw += v;
+    for (double& v : *w) v /= sw;
+}
+
+// Partially coherent envelope constants of the objective lens (PCTF_TEM, lens_modulation.cuh:
+// 91-110): temporal-only drops the source divergence, spatial-only the defocus spread;
+// dsf_iehwgd = sqrt(2) dsf_sigma (lens_dev.cuh:138-142).
+void set_pctf(LensDev* d, const ms_params& p, double lambda)
+{
+    const ms_lens& L = p.obj_lens;
+    const int tsi = p.temporal_spatial_incoh ? p.temporal_spatial_incoh : MS_TSI_TEMPORAL_SPATIAL;
+    const double beta = tsi == MS_TSI_TEMPORAL ? 0.0 : L.ssf_beta;
+    const double D = tsi == MS_TSI_SPATIAL ? 0.0 : std::sqrt(2.0) * L.dsf_sigma;
+    d->pctf = 1;
+    d->pe_a = kPi * beta * D;
+    d->pe_b = kPi * D * lambda;
+    d->pe_c = kPi * beta;
+    d->pe_d = L.c30 * lambda * lambda;
+    d->pe_e = L.c10;
 }
 
 struct Setup {
@@ -623,9 +680,53 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_STEP, pa, nw, p.nx, st);
         }
-        if (!kspace) {
-            // OL_modulation -> CTF_TEM (wave_function.cuh:96-110, lens_modulation.cuh:78-89)
+        const int illum = p.illumination_model ? p.illumination_model : MS_ILLUM_COHERENT;
+        const int tsi = p.temporal_spatial_incoh ? p.temporal_spatial_incoh : MS_TSI_TEMPORAL_SPATIAL;
+        if (!kspace && illum == MS_ILLUM_TCC && tsi != MS_TSI_COHERENT) {
+            // TCC_TEM (lens_modulation.cuh:130-176): every (source point, defocus node) pair images a
+            // copy of the exit wave; intensities (or complex fields) add with the quadrature weights
+            const ms_lens& OL = p.obj_lens;
+            std::vector<double> xt, wt, xs, ws;
+            gauss_hermite(tsi == MS_TSI_SPATIAL ? 1 : OL.dsf_npoints, &xt, &wt);
+            gauss_hermite(tsi == MS_TSI_TEMPORAL ? 1 : OL.ssf_npoints, &xs, &ws);
+            const double df_hw = std::sqrt(2.0) * OL.dsf_sigma;        // dsf_iehwgd
+            const double sf_hw = std::sin(OL.ssf_beta) / s.ph.lambda;  // ssf_iehwgd (lens_dev.cuh:143-148)
+            float2* q = (float2*)c->buf("tcc_q", sizeof(float2) * N * nw);
+            float2* aux = full ? (float2*)c->buf("aux", sizeof(float2) * N * nw) : nullptr;
+            float* img = full ? nullptr : (float*)c->buf("img_w", sizeof(float) * N * nw);
+            bool firstq = true;
+            for (size_t iy = 0; iy < xs.size(); iy++)
+                for (size_t ix = 0; ix < xs.size(); ix++)
+                    for (size_t j = 0; j < xt.size(); j++) {
+                        const double wq = ws[ix] * ws[iy] * wt[j];
+                        LensDev Lq = lens_dev(lens_coef(OL, s.ph.lambda, df_hw * xt[j]));
+                        Lq.gxu = sf_hw * xs[ix];
+                        Lq.gyu = sf_hw * xs[iy];
+                        Lq.amp = full ? wq : std::sqrt(wq);
+                        CK(cudaMemcpyAsync(q, psi, sizeof(float2) * N * nw, cudaMemcpyDeviceToDevice, st));
+                        PassArgs pq = pa;
+                        pq.psi = q;
+                        pq.lens = Lq;
+                        pq.tw = s.tw_y;
+                        run_col(c, p.ny, COL_CTF_INV, pq, nw, p.nx, st);
+                        pq.tw = s.tw_x;
+                        if (full) {
+                            pq.aux = aux;
+                            run_row(c, p.nx, ROW_INV_STORE, pq, nw, p.ny, st);
+                            launch_acc_cplx(aux, nw, dwv, N, acc, acc_im, first && firstq, st);
+                        } else {
+                            pq.out_real = img;
+                            pq.flags = firstq ? 0 : PF_ACCUMULATE;
+                            run_row(c, p.nx, ROW_INV_ABS2, pq, nw, p.ny, st);
+                        }
+                        firstq = false;
+                    }
+            if (!full) launch_acc_real(img, nw, N, acc, first, st);
+        } else if (!kspace) {
+            // OL_modulation -> CTF_TEM (wave_function.cuh:96-110, lens_modulation.cuh:78-89), or
+            // PCTF_TEM (:91-110) with the partially coherent envelope
             pa.lens = obj;
+            if (illum == MS_ILLUM_PARTIAL) set_pctf(&pa.lens, p, s.ph.lambda);
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_CTF_INV, pa, nw, p.nx, st);
             pa.tw = s.tw_x;

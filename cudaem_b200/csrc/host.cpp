@@ -359,8 +359,16 @@ void validate_params(const ms_params& p)
     MS_REQUIRE(p.E0 > 0 && p.E0 < 10000, MS_ERR_INVALID_ARG, "E0 must be in (0, 10000) kV");
     MS_REQUIRE(std::fabs(p.theta) < 1.0, MS_ERR_INVALID_ARG, "beam tilt theta out of range");
     MS_REQUIRE(p.enable_fine_slicing == 0, MS_ERR_UNSUPPORTED, "fine slicing is not implemented");
-    MS_REQUIRE(p.illumination_model == MS_ILLUM_COHERENT || p.illumination_model == 0, MS_ERR_UNSUPPORTED,
-               "only the coherent illumination model is implemented");
+    MS_REQUIRE(p.illumination_model == 0 || (p.illumination_model >= MS_ILLUM_COHERENT && p.illumination_model <= MS_ILLUM_TCC),
+               MS_ERR_INVALID_ARG, "illumination_model must be coherent, partial or TCC");
+    MS_REQUIRE(p.temporal_spatial_incoh >= 0 && p.temporal_spatial_incoh <= MS_TSI_COHERENT, MS_ERR_INVALID_ARG,
+               "temporal_spatial_incoh must be 1..4 (0 selects 1)");
+    MS_REQUIRE(p.obj_lens.dsf_sigma >= 0 && p.obj_lens.ssf_beta >= 0 && p.obj_lens.ssf_beta < 0.5, MS_ERR_INVALID_ARG,
+               "defocus spread and source divergence must be non-negative");
+    MS_REQUIRE(p.illumination_model != MS_ILLUM_TCC ||
+                   (p.obj_lens.dsf_npoints >= 1 && p.obj_lens.dsf_npoints <= 64 && p.obj_lens.ssf_npoints >= 1 &&
+                    p.obj_lens.ssf_npoints <= 16),
+               MS_ERR_INVALID_ARG, "TCC needs 1..64 defocus and 1..16 source quadrature points per axis");
     MS_REQUIRE(p.gpu_num <= 1, MS_ERR_UNSUPPORTED, "one GPU per context: gpu_num must be 1");
     MS_REQUIRE(p.phonon_model == MS_PHONON_STILL || p.phonon_model == MS_PHONON_FROZEN, MS_ERR_INVALID_ARG,
                "phonon_model must be still or frozen");

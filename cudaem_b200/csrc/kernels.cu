@@ -318,15 +318,26 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
             conj_all(v);
         }
     } else if constexpr (OP == COL_CTF_INV) {
-        // apply_CTF_kernel (device_kernels.cuh:445-468)
-        const double gx = freq_d(col, nx, a.grid.dgx);
+        // apply_CTF_kernel (device_kernels.cuh:445-468) with the source-point shift (gxu, gyu) and
+        // amplitude of a TCC quadrature point, or apply_PCTF_kernel (:505-518) with the partially
+        // coherent envelope (incoherent_phase_shift, basic_functions_dev.cuh:235-268)
+        const double gx = freq_d(col, nx, a.grid.dgx) + a.lens.gxu;
+        const float gxu = (float)a.lens.gxu, gyu = (float)a.lens.gyu;
 #pragma unroll
         for (int j = 0; j < E; j++) {
             const int k = g + G * j;
-            float g2 = det_g2(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f);
+            float g2 = det_g2_shift(col, k, nx, N, a.grid.dgx_f, a.grid.dgy_f, gxu, gyu);
             if (a.lens.g2min <= g2 && g2 < a.lens.g2max) {
-                double gy = freq_d(k, N, a.grid.dgy);
-                v[j] = cmul(v[j], expi_d(chi_d(a.lens, a.lens.cc10, gx, gy)));
+                double gy = freq_d(k, N, a.grid.dgy) + a.lens.gyu;
+                double amp = a.lens.amp;
+                if (a.lens.pctf) {
+                    const double gg = gx * gx + gy * gy;
+                    const double u = 1.0 + 2.0 * a.lens.pe_a * a.lens.pe_a * gg;
+                    const double ct = a.lens.pe_b * gg;
+                    const double cs = a.lens.pe_c * (a.lens.pe_d * gg - a.lens.pe_e);
+                    amp *= exp(-(cs * cs * gg + 0.5 * ct * ct) / u) / sqrt(u);
+                }
+                v[j] = cmul(v[j], cscale(expi_d(chi_d(a.lens, a.lens.cc10, gx, gy)), (float)amp));
             } else {
                 v[j] = make_float2(0.0f, 0.0f);
             }

@@ -33,6 +33,12 @@ struct LensDev {
     double cc10, cc12, cc21, cc23, cc30, cc32, cc34, cc41, cc43, cc45, cc50, cc52, cc54, cc56;
     double p12, p21, p23, p32, p34, p41, p43, p45, p52, p54, p56;
     float g2min, g2max;
+    // image-forming lens only (COL_CTF_INV): frequency shift of a source point, amplitude
+    // factor, and the partially coherent envelope (pctf = 1) with
+    // pe_a = pi beta D, pe_b = pi D lambda, pe_c = pi beta, pe_d = C30 lambda^2, pe_e = C10
+    double gxu, gyu, amp;
+    int pctf;
+    double pe_a, pe_b, pe_c, pe_d, pe_e;
 };
 
 enum RowOp {

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define MS_ABI_VERSION 1
+#define MS_ABI_VERSION 2
 #define MS_NR 128        /* radial spline nodes; c_nR in the reference (basic_functions_dev.cuh:51-65) */
 #define MS_MAX_DET 8     /* annular detectors per simulation */
 #define MS_MAX_COEF 6    /* linear / non-linear coefficients per element parameterisation */
@@ -64,8 +64,12 @@ enum {
     MS_POT_DOYLE_0_4 = 1, MS_POT_PENG_0_4 = 2, MS_POT_PENG_0_12 = 3, MS_POT_KIRKLAND_0_12 = 4,
     MS_POT_WEICKENMEIER_0_12 = 5, MS_POT_LOBATO_0_12 = 6, MS_POT_MOLIERE = 7
 };
-/* eIllumination_Model (lens_modulation.cuh:34-54); only coherent is implemented */
+/* eIllumination_Model (lens_modulation.cuh:34-54): coherent CTF, partially coherent CTF
+ * (envelope, PCTF_TEM :91-110) or transmission cross-coefficient quadrature (TCC_TEM :130-176);
+ * the last two apply to the HRTEM image */
 enum { MS_ILLUM_COHERENT = 1, MS_ILLUM_PARTIAL = 2, MS_ILLUM_TCC = 3 };
+/* eTemporal_Spatial_Incoh (multislice_params_dev.cuh:27) */
+enum { MS_TSI_TEMPORAL_SPATIAL = 1, MS_TSI_TEMPORAL = 2, MS_TSI_SPATIAL = 3, MS_TSI_COHERENT = 4 };
 /* data_record (multislice_params_dev.cuh:117): intensity or full complex wave */
 enum { MS_RECORD_INTENSITY = 0, MS_RECORD_WAVE = 1 };
 /* execution form of the STEM scan: batched probes (tile scan) or one probe per launch (general scan) */
@@ -81,6 +85,11 @@ typedef struct ms_lens {
     double c41, phi41, c43, phi43, c45, phi45;
     double c50, c52, phi52, c54, phi54, c56, phi56;
     double inner_aper_ang, outer_aper_ang;   /* aperture semi-angles, rad */
+    /* partial coherence of the objective lens (lens_dev.cuh:27-34) */
+    double dsf_sigma;                        /* standard deviation of the defocus spread, Angstrom */
+    double ssf_beta;                         /* source divergence semi-angle, rad */
+    int dsf_npoints;                         /* TCC: defocus quadrature points (Gauss-Hermite) */
+    int ssf_npoints;                         /* TCC: source quadrature points per axis (Gauss-Hermite) */
 } ms_lens;
 
 /* One element's V(r) parameterisation: the cl/cnl tables of Element_Coeffs
@@ -127,7 +136,8 @@ typedef struct ms_params {
     double iw_x, iw_y;            /* probe position in the specimen frame, Angstrom */
     ms_lens cond_lens;            /* condenser lens: the probe */
     ms_lens obj_lens;             /* objective lens: the HRTEM image */
-    int illumination_model;       /* MS_ILLUM_COHERENT */
+    int illumination_model;       /* MS_ILLUM_* */
+    int temporal_spatial_incoh;   /* MS_TSI_*: which spreads the partial-coherence models include */
     int data_record;              /* MS_RECORD_* */
     int scan_nx, scan_ny;         /* STEM scan size (columns, rows) */
     double scan_x0, scan_y0;      /* first probe position, Angstrom */

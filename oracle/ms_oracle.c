@@ -823,6 +823,91 @@ static void or_confs(const ms_params* p, int* c0, int* c1, double* w)
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* partial coherence of the objective lens                                   */
+/* ------------------------------------------------------------------------ */
+/* Gauss-Hermite nodes and weights for the weight exp(-x^2), n points, weights normalised to
+   sum 1.  The reference's quadrature tables (output_qt / output_qs of the missing
+   multislice_params.hpp) are not shipped; this is the standard Newton iteration on the
+   orthonormal Hermite recurrence (Golub and Welsch give the same nodes), with the usual
+   asymptotic starting points. */
+void or_gauss_hermite(int n, double* x, double* w)
+{
+    const double pim4 = 0.7511255444649425; /* pi^(-1/4) */
+    double z = 0.0, pp = 0.0;
+    int m = (n + 1) / 2;
+    for (int i = 0; i < m; i++) {
+        if (i == 0) z = sqrt(2.0 * n + 1.0) - 1.85575 * pow(2.0 * n + 1.0, -0.16667);
+        else if (i == 1) z -= 1.14 * pow((double)n, 0.426) / z;
+        else if (i == 2) z = 1.86 * z - 0.86 * x[0];
+        else if (i == 3) z = 1.91 * z - 0.91 * x[1];
+        else z = 2.0 * z - x[i - 2];
+        for (int it = 0; it < 100; it++) {
+            double p1 = pim4, p2 = 0.0;
+            for (int j = 1; j <= n; j++) {
+                double p3 = p2;
+                p2 = p1;
+                p1 = z * sqrt(2.0 / j) * p2 - sqrt((double)(j - 1) / j) * p3;
+            }
+            pp = sqrt(2.0 * n) * p2;
+            double z1 = z;
+            z = z1 - p1 / pp;
+            if (fabs(z - z1) <= 1e-15 * (1.0 + fabs(z))) break;
+        }
+        x[i] = z;
+        x[n - 1 - i] = -z;
+        w[i] = 2.0 / (pp * pp);
+        w[n - 1 - i] = w[i];
+    }
+    if (n % 2 == 1) x[m - 1] = 0.0;
+    double sw = 0.0;
+    for (int i = 0; i < n; i++) sw += w[i];
+    for (int i = 0; i < n; i++) w[i] /= sw;
+}
+
+/* partially coherent envelope (incoherent_phase_shift, basic_functions_dev.cuh:235-268),
+   dsf_iehwgd = sqrt(2) dsf_sigma (lens_dev.cuh:138-142); temporal-only zeroes the source
+   divergence, spatial-only the defocus spread (PCTF_TEM, lens_modulation.cuh:91-110) */
+static double or_pctf_env(const ms_params* p, double lambda, double g2)
+{
+    const ms_lens* L = &p->obj_lens;
+    int tsi = p->temporal_spatial_incoh ? p->temporal_spatial_incoh : MS_TSI_TEMPORAL_SPATIAL;
+    double beta = (tsi == MS_TSI_TEMPORAL) ? 0.0 : L->ssf_beta;
+    double df = (tsi == MS_TSI_SPATIAL) ? 0.0 : sqrt(2.0) * L->dsf_sigma;
+    double c = OR_PI * beta * df;
+    double u = 1.0 + 2.0 * c * c * g2;
+    c = OR_PI * df * lambda * g2;
+    double temp_inc = 0.5 * c * c;
+    c = OR_PI * beta * (L->c30 * lambda * lambda * g2 - L->c10);
+    double spa_inc = c * c * g2;
+    return exp(-(spa_inc + temp_inc) / u) / sqrt(u);
+}
+
+/* the image-forming lens on an exit wave in reciprocal space: apply_CTF_kernel (device_kernels.cuh:
+   445-468) with the frequency shift (gxu, gyu), the optional envelope, and an amplitude factor;
+   then the inverse FFT.  out may be W itself (the update is element by element). */
+static void or_ctf_image(const ms_params* p, const or_sim* s, const or_lens* L, double gxu, double gyu, int pctf,
+                         double amp, const cplx* W, cplx* out)
+{
+    float gxuf = (float)gxu, gyuf = (float)gyu;
+    for (int iy = 0; iy < s->ny; iy++)
+        for (int ix = 0; ix < s->nx; ix++) {
+            size_t k = (size_t)iy * s->nx + ix;
+            float gxf = (float)or_fshift(ix, s->nx) * s->dgx_f + gxuf;
+            float gyf = (float)or_fshift(iy, s->ny) * s->dgy_f + gyuf;
+            float g2 = gxf * gxf + gyf * gyf;
+            if (L->g2min <= g2 && g2 < L->g2max) {
+                double gx = or_fshift(ix, s->nx) * s->dgx + gxu, gy = or_fshift(iy, s->ny) * s->dgy + gyu;
+                double ch = or_chi(L, gx, gy);
+                double a = amp;
+                if (pctf) a *= or_pctf_env(p, s->lambda, gx * gx + gy * gy);
+                out[k] = W[k] * a * (cos(ch) + I * sin(ch));
+            } else
+                out[k] = 0.0;
+        }
+    or_fft2c(out, s->nx, s->ny, +1);
+}
+
 /* ED_HRTEM (single_simulator.cuh:11-126) and CBED_CBEI (:128-206) */
 static int or_tem_like(const ms_params* p, const ms_atoms* a, double* img, double* re, double* im, int kspace)
 {
@@ -845,22 +930,44 @@ static int or_tem_like(const ms_params* p, const ms_atoms* a, double* img, doubl
         or_spec_build(p, a, c, &sp);
         or_incident(p, &s, p->iw_x, p->iw_y, sp.z_init, wv);
         or_multislice(&s, wv, NULL, sp.ns, P, p, a, &sp, es, Vt);
+        int tsi = p->temporal_spatial_incoh ? p->temporal_spatial_incoh : MS_TSI_TEMPORAL_SPATIAL;
+        if (!kspace && p->illumination_model == MS_ILLUM_TCC && tsi != MS_TSI_COHERENT) {
+            /* TCC_TEM (lens_modulation.cuh:130-176): incoherent sum over the defocus quadrature
+               (c10 + dsf_iehwgd x_j) and the source quadrature (frequency shift qs_i) */
+            const ms_lens* OL = &p->obj_lens;
+            int nt = (tsi == MS_TSI_SPATIAL) ? 1 : OL->dsf_npoints;
+            int ns1 = (tsi == MS_TSI_TEMPORAL) ? 1 : OL->ssf_npoints;
+            double xt[64], wt[64], xs[16], ws[16];
+            if (nt == 1) { xt[0] = 0.0; wt[0] = 1.0; } else or_gauss_hermite(nt, xt, wt);
+            if (ns1 == 1) { xs[0] = 0.0; ws[0] = 1.0; } else or_gauss_hermite(ns1, xs, ws);
+            double df_hw = sqrt(2.0) * OL->dsf_sigma;               /* dsf_iehwgd */
+            double sf_hw = sin(OL->ssf_beta) / s.lambda;            /* ssf_iehwgd (lens_dev.cuh:143-148) */
+            cplx* tmp = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+            for (int iy_s = 0; iy_s < ns1; iy_s++)
+                for (int ix_s = 0; ix_s < ns1; ix_s++)
+                    for (int j = 0; j < nt; j++) {
+                        double wq = ws[ix_s] * ws[iy_s] * wt[j];
+                        or_lens L;
+                        or_lens_init(OL, s.lambda, df_hw * xt[j], &L);
+                        or_ctf_image(p, &s, &L, sf_hw * xs[ix_s], sf_hw * xs[iy_s], 0, 1.0, wv, tmp);
+                        for (long k = 0; k < s.N; k++) {
+                            if (full) {
+                                re[k] += w * wq * creal(tmp[k]);
+                                im[k] += w * wq * cimag(tmp[k]);
+                            } else
+                                img[k] += w * wq * (creal(tmp[k]) * creal(tmp[k]) + cimag(tmp[k]) * cimag(tmp[k]));
+                        }
+                    }
+            free(tmp);
+            or_spec_free(&sp);
+            continue;
+        }
         if (!kspace) {
-            /* OL_modulation -> CTF_TEM (lens_modulation.cuh:78-89): apply_CTF_kernel, inverse FFT */
+            /* OL_modulation -> CTF_TEM (lens_modulation.cuh:78-89) or PCTF_TEM (:91-110):
+               apply_CTF_kernel / apply_PCTF_kernel, inverse FFT */
             or_lens L;
             or_lens_init(&p->obj_lens, s.lambda, 0.0, &L);
-            for (int iy = 0; iy < s.ny; iy++)
-                for (int ix = 0; ix < s.nx; ix++) {
-                    size_t k = (size_t)iy * s.nx + ix;
-                    float g2 = or_g2f(&s, ix, iy);
-                    if (L.g2min <= g2 && g2 < L.g2max) {
-                        double gx = or_fshift(ix, s.nx) * s.dgx, gy = or_fshift(iy, s.ny) * s.dgy;
-                        double ch = or_chi(&L, gx, gy);
-                        wv[k] *= cos(ch) + I * sin(ch);
-                    } else
-                        wv[k] = 0.0;
-                }
-            or_fft2c(wv, s.nx, s.ny, +1);
+            or_ctf_image(p, &s, &L, 0.0, 0.0, p->illumination_model == MS_ILLUM_PARTIAL, 1.0, wv, wv);
         }
         for (long k = 0; k < s.N; k++) {
             if (full) {

@@ -61,6 +61,9 @@ int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_
                      const double* probe_xy, int n_probe, const float* target, double* loss,
                      double* dL_dV, double* dL_dC10, double* dL_dC30);
 
+/* Gauss-Hermite quadrature for exp(-x^2), weights normalised to sum 1 */
+void or_gauss_hermite(int n, double* x, double* w);
+
 /* number of OpenMP threads the oracle uses (0 = runtime default) */
 void or_set_threads(int n);
 int or_get_threads(void);

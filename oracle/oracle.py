@@ -49,6 +49,7 @@ def lib() -> C.CDLL:
             "or_simulate_thickness": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), C.c_int64, P(i)]),
             "or_stem_forward_potential": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(d)]),
             "or_stem_backward": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(f), P(d), P(d), P(d), P(d)]),
+            "or_gauss_hermite": (None, [i, P(d), P(d)]),
             "or_set_threads": (None, [i]),
             "or_get_threads": (i, []),
         }
@@ -203,3 +204,9 @@ def stem_backward(params, V, z_init, xy, target):
     lib().or_stem_backward(C.byref(p), _f(V), V.shape[0], z_init, _d(xy), xy.shape[0], _f(T), C.byref(loss),
                            _d(gV), C.byref(g10), C.byref(g30))
     return loss.value, gV, g10.value, g30.value
+
+
+def gauss_hermite(n: int):
+    x, w = np.empty(n), np.empty(n)
+    lib().or_gauss_hermite(n, _d(x), _d(w))
+    return x, w

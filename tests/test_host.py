@@ -86,7 +86,8 @@ def test_crystal_builder():
 @pytest.mark.parametrize("field,value,status", [
     ("nx", 100, abi.MS_ERR_UNSUPPORTED), ("ny", 4096, abi.MS_ERR_UNSUPPORTED), ("dz", 0.0, abi.MS_ERR_INVALID_ARG),
     ("E0", -1.0, abi.MS_ERR_INVALID_ARG), ("enable_fine_slicing", 1, abi.MS_ERR_UNSUPPORTED),
-    ("illumination_model", abi.MS_ILLUM_TCC, abi.MS_ERR_UNSUPPORTED), ("gpu_num", 2, abi.MS_ERR_UNSUPPORTED),
+    ("illumination_model", 9, abi.MS_ERR_INVALID_ARG), ("temporal_spatial_incoh", 7, abi.MS_ERR_INVALID_ARG),
+    ("gpu_num", 2, abi.MS_ERR_UNSUPPORTED),
     ("n_det", 9, abi.MS_ERR_INVALID_ARG), ("phonon_model", 2, abi.MS_ERR_INVALID_ARG),
     ("simulation_type", 9, abi.MS_ERR_INVALID_ARG)])
 def test_validation_status_codes(field, value, status):
@@ -116,15 +117,36 @@ def test_header_symbols_exported():
     for s in sorted(decl):
         assert hasattr(L, s), s
         assert s in abi.PROTOTYPES, s
-    assert L.ms_abi_version() == 1
+    assert L.ms_abi_version() == 2
     assert b"sm_100a" in L.ms_version()
 
 
-def test_struct_layouts():
-    """ctypes mirrors match the C layout (size of the params struct is fixed by the header)."""
-    assert C.sizeof(abi.ms_lens) == 8 + 27 * 8
-    assert C.sizeof(abi.ms_atoms) == 7 * 8
-    assert C.sizeof(abi.ms_element_coef) == 8 + 12 * 8
+def test_struct_layouts(tmp_path):
+    """The ctypes mirrors match the C layout of include/cudaem_b200.h field by field: a small C
+    program compiled from the header prints every struct's size and every field's offset."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = [abi.ms_lens, abi.ms_element_coef, abi.ms_atoms, abi.ms_params, abi.ms_output]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "cudaem_b200.h"', "int main(void) {"]
+    expect = []
+    for st in structs:
+        nm = st.__name__
+        lines.append(f'printf("%zu\\n", sizeof({nm}));')
+        expect.append(C.sizeof(st))
+        for f in st._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({nm}, {f[0]}));')
+            expect.append(getattr(st, f[0]).offset)
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == expect
 
 
 def test_no_device_is_reported():

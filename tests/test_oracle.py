@@ -162,3 +162,20 @@ def test_adjoint_matches_finite_differences():
         fd = (L(V, qp) - L(V, qm)) / (2 * h)
         assert abs(fd - g) / abs(g) < 1e-4
     del rng
+
+
+def test_gauss_hermite_known_answers():
+    """Quadrature of the partial-coherence models: exact nodes for n = 2, 3 and exact moments of
+    exp(-x^2) (normalised: <x^2> = 1/2, <x^4> = 3/4, <x^6> = 15/8) up to degree 2n-1."""
+    x, w = orc.gauss_hermite(2)
+    assert np.allclose(np.sort(x), [-np.sqrt(0.5), np.sqrt(0.5)], atol=1e-14) and np.allclose(w, 0.5)
+    x, w = orc.gauss_hermite(3)
+    assert np.allclose(np.sort(x), [-np.sqrt(1.5), 0.0, np.sqrt(1.5)], atol=1e-14)
+    assert np.allclose(w[np.argsort(x)], [1 / 6, 2 / 3, 1 / 6], atol=1e-14)
+    for n in (4, 8, 16, 40, 64):
+        x, w = orc.gauss_hermite(n)
+        assert abs(w.sum() - 1) < 1e-13
+        assert abs(np.dot(w, x ** 2) - 0.5) < 1e-12
+        assert abs(np.dot(w, x ** 4) - 0.75) < 1e-11
+        assert abs(np.dot(w, x ** 6) - 15 / 8) < 1e-10
+        assert abs(np.dot(w, x ** 3)) < 1e-12
