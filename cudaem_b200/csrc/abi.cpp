@@ -114,6 +114,8 @@ ms_status ms_destroy(ms_ctx* c)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (auto s : c->side) cudaStreamDestroy(s);
+    if (c->pot_stream) cudaStreamDestroy(c->pot_stream);
+    for (auto e : c->chunk_ev) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return MS_OK;

@@ -39,6 +39,8 @@ struct ms_ctx {
     int pass_variant = 0;                        // msb::PassVariant of the slice-pass kernels (0: classic)
     int last_batch = 0;                          // probe batch used by the last STEM call
     std::vector<cudaStream_t> side;              // streams of the grid groups of an uneven batch
+    cudaStream_t pot_stream = nullptr;           // potential chunks computed beside the slice passes
+    std::vector<cudaEvent_t> chunk_ev;           // completion of each potential chunk
     std::map<std::string, int> batch_choice;     // autotuned probe batch per grid and slice count
     void drop_graph();
 

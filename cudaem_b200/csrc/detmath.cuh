@@ -176,6 +176,18 @@ MS_HD int det_slice_of(float zk, const float* b, int nv, float vmax)
     return -1;
 }
 
+// Fine slicing: does slice [zs, ze) integrate the atom at height z?  Its integration range is
+// [min(z_m - R, zs), max(z_m + R, ze)] grown by the slicing epsilon, with z_m the slice middle
+// (get_slicing and fd_by_z with Inc_Borders, slice_generator.hpp:78-129): z >= lower and
+// (z < upper, or the highest atom lies at or below upper).
+MS_HD bool det_fine_member(float z, float zs, float ze, float rint, float zmax)
+{
+    const float zm = MSF_MUL(0.5f, MSF_ADD(zs, ze));
+    const float lo = MSF_SUB(fminf(MSF_SUB(zm, rint), zs), kSliceEps);
+    const float hi = MSF_ADD(fmaxf(MSF_ADD(zm, rint), ze), kSliceEps);
+    return z >= lo && (z < hi || zmax <= hi);
+}
+
 // Frequency of FFT index i on an n-point axis, as float (grid_dev.cuh:429-444).
 MS_HD float det_gfreq(int i, int n, float dg)
 {

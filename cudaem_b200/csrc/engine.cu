@@ -21,6 +21,7 @@
 #include "detmath.cuh"
 #include "fft_layout.hpp"
 #include "kernels.cuh"
+#include "vr.cuh"
 
 #define CK(x)                                                                                              \
     do {                                                                                                   \
@@ -333,6 +334,7 @@ struct AtomsDev {
     const float *x, *y, *z, *sig, *occ;
     const int* elem;
     const ElemTable* tables;
+    const ElemCoefDev* coefs;   // V(r) coefficients per element (fine slicing)
     int n_elem;
     float rmax_all;   // largest cut-off radius over the elements
 };
@@ -354,9 +356,17 @@ AtomsDev upload_atoms(ms_ctx* c, const ms_params& p, const ms_atoms& a)
 {
     AtomsDev d;
     d.n = a.n;
-    std::vector<int> zs(a.Z, a.Z + a.n);
-    std::sort(zs.begin(), zs.end());
-    zs.erase(std::unique(zs.begin(), zs.end()), zs.end());
+    // distinct atomic numbers in ascending order, and each atom's index among them, in O(n)
+    // (Z is validated to 1..103)
+    int zmap[128];
+    std::fill(zmap, zmap + 128, -1);
+    for (int64_t i = 0; i < a.n; i++) zmap[a.Z[i] & 127] = 0;
+    std::vector<int> zs;
+    for (int z = 0; z < 128; z++)
+        if (zmap[z] >= 0) {
+            zmap[z] = (int)zs.size();
+            zs.push_back(z);
+        }
     MS_REQUIRE(zs.size() <= 16, MS_ERR_UNSUPPORTED, "at most 16 distinct elements per specimen");
     std::vector<ElemTable> tabs(zs.size());
     for (size_t i = 0; i < zs.size(); i++) {
@@ -370,7 +380,7 @@ AtomsDev upload_atoms(ms_ctx* c, const ms_params& p, const ms_atoms& a)
         tabs[i] = it->second;
     }
     std::vector<int> el(a.n);
-    for (int64_t i = 0; i < a.n; i++) el[i] = (int)(std::lower_bound(zs.begin(), zs.end(), a.Z[i]) - zs.begin());
+    for (int64_t i = 0; i < a.n; i++) el[i] = zmap[a.Z[i] & 127];
     size_t fb = sizeof(float) * (size_t)a.n;
     float* x = (float*)c->buf("at_x", fb);
     float* y = (float*)c->buf("at_y", fb);
@@ -386,6 +396,11 @@ AtomsDev upload_atoms(ms_ctx* c, const ms_params& p, const ms_atoms& a)
     CK(cudaMemcpyAsync(oc, a.occ, fb, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(e, el.data(), sizeof(int) * (size_t)a.n, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(t, tabs.data(), sizeof(ElemTable) * tabs.size(), cudaMemcpyHostToDevice, c->stream));
+    std::vector<ElemCoefDev> cf(zs.size());
+    for (size_t i = 0; i < zs.size(); i++) cf[i] = elem_coef_dev(p, zs[i]);
+    ElemCoefDev* dcf = (ElemCoefDev*)c->buf("at_coef", sizeof(ElemCoefDev) * cf.size());
+    CK(cudaMemcpyAsync(dcf, cf.data(), sizeof(ElemCoefDev) * cf.size(), cudaMemcpyHostToDevice, c->stream));
+    d.coefs = dcf;
     d.x = x; d.y = y; d.z = z; d.sig = sg; d.occ = oc; d.elem = e; d.tables = t;
     d.n_elem = (int)tabs.size();
     d.rmax_all = 0.f;
@@ -404,6 +419,7 @@ struct SpecGroup {
     const int* ae = nullptr;
     const unsigned* seg = nullptr;
     const int* ns_d = nullptr;
+    const float4* pair_coef = nullptr;   // fine slicing: per-pair spline coefficients
     CellGrid cg;
 };
 
@@ -444,9 +460,14 @@ SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const
     g.ns.resize(nc);
     g.z_init.resize(nc);
     int S_cap = 1;
+    const bool fine = p.enable_fine_slicing != 0;
+    const float rint = fine ? fine_radius(p) : 0.0f;
+    // the planes' range: the atoms' z range, grown by the integration radius under fine slicing
+    auto plane_lo = [&](float lo) { return fine ? MSF_SUB(lo, rint) : lo; };
+    auto plane_hi = [&](float hi) { return fine ? MSF_ADD(hi, rint) : hi; };
     for (int i = 0; i < nc; i++) {
         float lo = ord2f(zh[i]), hi = ord2f(zh[nc + i]);
-        nv[i] = det_nplanes(lo, hi, dz);
+        nv[i] = det_nplanes(plane_lo(lo), plane_hi(hi), dz);
         vmax[i] = hi;
         g.ns[i] = nv[i] - 1;
         S_cap = std::max(S_cap, g.ns[i]);
@@ -456,7 +477,8 @@ SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const
     std::vector<float> bounds((size_t)nc * bstride, 0.0f);
     for (int i = 0; i < nc; i++) {
         float lo = ord2f(zh[i]), hi = ord2f(zh[nc + i]);
-        for (int k = 0; k < nv[i]; k++) bounds[(size_t)i * bstride + k] = det_plane(k, nv[i], lo, hi, dz, border);
+        for (int k = 0; k < nv[i]; k++)
+            bounds[(size_t)i * bstride + k] = det_plane(k, nv[i], plane_lo(lo), plane_hi(hi), dz, border);
         float sum = bounds[(size_t)i * bstride] + bounds[(size_t)i * bstride + 1];
         g.z_init[i] = (double)(float)(0.5 * (double)sum);  // Slice::z_m (slice.hpp:19-22)
     }
@@ -481,7 +503,9 @@ SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const
     const int64_t nkeys64 = nc * (S_cap + 1) * (int64_t)g.cg.ncx * g.cg.ncy;
     MS_REQUIRE(nkeys64 < (1LL << 31), MS_ERR_UNSUPPORTED, "too many (configuration, slice, cell) bins");
     const int nkeys = (int)nkeys64;
-    const int64_t total = n * nc;
+    // fine slicing: up to maxper (atom, slice) pairs per atom, unused slots keyed past every bin
+    const int maxper = fine ? (int)std::ceil(2.0 * rint / dz) + 4 : 1;
+    const int64_t total = n * nc * maxper;
     MS_REQUIRE(total < (1LL << 31), MS_ERR_UNSUPPORTED, "atoms x configurations must stay below 2^31 per group");
     unsigned* keys = (unsigned*)c->buf("sp_keys", sizeof(unsigned) * total);
     unsigned* keys2 = (unsigned*)c->buf("sp_keys2", sizeof(unsigned) * total);
@@ -489,9 +513,13 @@ SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const
     int* vals2 = (int*)c->buf("sp_vals2", sizeof(int) * total);
     unsigned* counts = (unsigned*)c->buf("sp_counts", sizeof(unsigned) * (nkeys + 1));
     CK(cudaMemsetAsync(counts, 0, sizeof(unsigned) * (nkeys + 1), st));
-    launch_assign(xd, yd, zd, n, (int)nc, db, bstride, dnv, dvmax, S_cap, g.cg, keys, vals, counts, st);
+    if (fine)
+        launch_fine_assign(xd, yd, zd, n, (int)nc, db, bstride, dnv, dvmax, S_cap, g.cg, rint, maxper,
+                           (unsigned)nkeys, keys, vals, counts, st);
+    else
+        launch_assign(xd, yd, zd, n, (int)nc, db, bstride, dnv, dvmax, S_cap, g.cg, keys, vals, counts, st);
     int end_bit = 1;
-    while ((1LL << end_bit) < nkeys) end_bit++;
+    while ((1LL << end_bit) <= nkeys) end_bit++;
     size_t tmp_bytes = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, vals2, (int)total, 0, end_bit, st));
     void* tmp = c->buf("sp_sorttmp", tmp_bytes);
@@ -505,8 +533,23 @@ SpecGroup build_specimen(ms_ctx* c, const ms_params& p, const AtomsDev& A, const
     float* ay = (float*)c->buf("sp_ay", sizeof(float) * total);
     float* aw = (float*)c->buf("sp_aw", sizeof(float) * total);
     int* ae = (int*)c->buf("sp_ae", sizeof(int) * total);
-    launch_gather(keys2, vals2, total, n, S_cap, g.cg, xd, yd, A.occ, A.elem, (float)ph.vr_factor, ax, ay, aw, ae,
-                  st);
+    if (fine) {
+        float* az = (float*)c->buf("sp_az", sizeof(float) * total);
+        launch_fine_gather(keys2, vals2, total, n, S_cap, g.cg, (unsigned)nkeys, xd, yd, zd, A.occ, A.elem,
+                           (float)ph.vr_factor, ax, ay, aw, ae, az, st);
+        // the z quadrature on [-1/2, 1/2] (nodes, then weights)
+        double* qz = (double*)c->buf("fine_qz", sizeof(double) * 2 * kNqz);
+        std::vector<double> q(2 * kNqz);
+        gauss_legendre_half(kNqz, q.data(), q.data() + kNqz);
+        CK(cudaMemcpyAsync(qz, q.data(), sizeof(double) * 2 * kNqz, cudaMemcpyHostToDevice, st));
+        float4* tab = (float4*)c->buf("sp_fine_tab", sizeof(float4) * MS_NR * total);
+        launch_fine_tables(keys2, az, ae, seg, (unsigned)nkeys, total, db, bstride, S_cap, g.cg, A.coefs,
+                           p.pot_rmin > 0 ? p.pot_rmin : 0.01, p.pot_rmax > 0 ? p.pot_rmax : 3.0, qz, tab, st);
+        g.pair_coef = tab;
+    } else {
+        launch_gather(keys2, vals2, total, n, S_cap, g.cg, xd, yd, A.occ, A.elem, (float)ph.vr_factor, ax, ay, aw,
+                      ae, st);
+    }
     g.ax = ax; g.ay = ay; g.aw = aw; g.ae = ae; g.seg = seg; g.ns_d = dns;
     return g;
 }
@@ -539,7 +582,64 @@ PotArgs pot_args(const ms_params& p, const Setup& s, const AtomsDev& A, const Sp
     a.wrap = p.pot_wrap ? 1 : 0;
     a.elems = A.tables;
     a.n_elem = A.n_elem;
+    a.pair_coef = g.pair_coef;
     return a;
+}
+
+// Potential chunks computed on a side stream (see sim_tem_like).
+constexpr int kPotChunk = 16;
+struct PotChunks {
+    std::vector<cudaEvent_t> ev;   // ev[k]: slices [k kPotChunk, (k+1) kPotChunk) are written
+    void wait(ms_ctx* c, int slice) const
+    {
+        if (slice % kPotChunk == 0 && slice > 0 && (size_t)(slice / kPotChunk) < ev.size() && ev[slice / kPotChunk])
+            CK(cudaStreamWaitEvent(c->stream, ev[slice / kPotChunk], 0));
+    }
+};
+
+cudaStream_t pot_stream(ms_ctx* c)
+{
+    if (!c->pot_stream) CK(cudaStreamCreateWithFlags(&c->pot_stream, cudaStreamNonBlocking));
+    return c->pot_stream;
+}
+
+cudaEvent_t chunk_event(ms_ctx* c, size_t k)
+{
+    while (c->chunk_ev.size() <= k) {
+        cudaEvent_t e = nullptr;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->chunk_ev.push_back(e);
+    }
+    return c->chunk_ev[k];
+}
+
+PotChunks launch_potential_chunks(ms_ctx* c, PotArgs a, int n_conf, int S)
+{
+    PotChunks pc;
+    const int nchunk = (S + kPotChunk - 1) / kPotChunk;
+    if (c->profile || nchunk <= 1) {
+        run_potential(c, a, n_conf, c->stream);
+        return pc;
+    }
+    pc.ev.assign((size_t)nchunk, nullptr);
+    // the side stream starts once the specimen (sorted atoms) is ready on the context stream
+    cudaEvent_t ready = chunk_event(c, 0);
+    CK(cudaEventRecord(ready, c->stream));
+    cudaStream_t side = pot_stream(c);
+    CK(cudaStreamWaitEvent(side, ready, 0));
+    PotArgs a0 = a;
+    a0.slice0 = 0;
+    a0.nslice = std::min(kPotChunk, S);
+    launch_potential(a0, n_conf, c->stream);
+    for (int k = 1; k < nchunk; k++) {
+        PotArgs ak = a;
+        ak.slice0 = k * kPotChunk;
+        ak.nslice = std::min(kPotChunk, S - k * kPotChunk);
+        launch_potential(ak, n_conf, side);
+        pc.ev[k] = chunk_event(c, (size_t)k);
+        CK(cudaEventRecord(pc.ev[k], side));
+    }
+    return pc;
 }
 
 PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const float* sV, int64_t slot_stride,
@@ -600,7 +700,16 @@ int estimate_slices(const ms_params& p, const ms_atoms& a)
         hi = std::max(hi, a.z[i]);
         smax = std::max(smax, a.sigma[i]);
     }
-    return (int)((hi - lo + 12.0f * smax) / (float)p.dz) + 3;
+    const float grow = p.enable_fine_slicing ? 2.0f * fine_radius(p) : 0.0f;
+    return (int)((hi - lo + 12.0f * smax + grow) / (float)p.dz) + 3;
+}
+
+// device bytes per configuration of the fine-slicing pair tables and sort buffers
+size_t fine_bytes_per_conf(const ms_params& p, const ms_atoms& a)
+{
+    if (!p.enable_fine_slicing) return 0;
+    const int maxper = (int)std::ceil(2.0 * fine_radius(p) / (float)p.dz) + 4;
+    return (size_t)a.n * maxper * (sizeof(float) * 4 * MS_NR + 48);
 }
 
 }  // namespace
@@ -639,7 +748,8 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
 
     // configurations per group: potential store + waves must fit the memory budget
     int S_est = estimate_slices(p, a);
-    size_t per_conf = (size_t)S_est * N * 4 + (size_t)N * 8 * 2 + (size_t)N * 4 + (size_t)a.n * 40;
+    size_t per_conf = (size_t)S_est * N * 4 + (size_t)N * 8 * 2 + (size_t)N * 4 + (size_t)a.n * 40 +
+                      fine_bytes_per_conf(p, a);
     int gsize = (int)std::max<size_t>(1, std::min<size_t>(cs.confs.size(), free_budget() / per_conf));
 
     double* acc = (double*)c->buf("acc0", sizeof(double) * N);
@@ -653,7 +763,11 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         const int nw = g.nconf;
         const int64_t slot = (int64_t)g.S_cap * N;
         float* sV = (float*)c->buf("sV", sizeof(float) * slot * nw);
-        run_potential(c, pot_args(p, s, A, g, sV, slot, 0, g.S_cap, 0), nw, st);
+        // Potentials in chunks of kPotChunk slices: the first on the context stream, the rest on a
+        // side stream, so that they are computed while the slice passes of earlier slices run (the
+        // passes are latency bound and leave issue slots free); the row pass of the first slice of
+        // each chunk waits for that chunk's event.  With per-launch profiling on, all run in order.
+        PotChunks pc = launch_potential_chunks(c, pot_args(p, s, A, g, sV, slot, 0, g.S_cap, 0), nw, g.S_cap);
         std::vector<WaveInfo> wv(nw);
         for (int i = 0; i < nw; i++) {
             wv[i].px = p.iw_x;
@@ -674,6 +788,7 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         }
         const int S_max = *std::max_element(g.ns.begin(), g.ns.end());
         for (int sl = 0; sl < S_max; sl++) {
+            pc.wait(c, sl);
             pa.slice = sl;
             pa.tw = s.tw_x;
             run_row(c, p.nx, (sl == 0 && iw == MS_IW_PLANE) ? ROW_T_FWD : ROW_INV_T_FWD, pa, nw, p.ny, st);

@@ -75,6 +75,14 @@ int iw_of(const ms_params& p);
 void host_displace(const ms_params& p, const ms_atoms& a, int conf, float* x, float* y, float* z);
 int host_slices(const ms_params& p, const float* z, int64_t n, std::vector<float>* bounds, int* atom_slice);
 
+// Fine slicing: the integration radius (the largest cut-off radius, atoms.R_int_max),
+// each element's coefficients for the device, and the z quadrature on [-1/2, 1/2].
+float fine_radius(const ms_params& p);
+struct ElemCoefDev;
+ElemCoefDev elem_coef_dev(const ms_params& p, int Z);
+void gauss_legendre_half(int n, double* x, double* w);
+constexpr int kNqz = 64;   // z quadrature points per slice (c_nqz)
+
 void validate_params(const ms_params& p);
 void validate_atoms(const ms_params& p, const ms_atoms* a);
 

@@ -9,6 +9,7 @@
 #include <thread>
 
 #include "detmath.cuh"
+#include "vr.cuh"
 #include "engine.hpp"
 
 namespace msb {
@@ -60,6 +61,8 @@ GridConst grid_of(const ms_params& p, const Physics& ph)
 }
 
 double gate_coef(double v) { return std::fabs(v) > 1e-5 ? v : 0.0; }
+
+float fine_radius(const ms_params& p) { return (float)(p.pot_rmax > 0 ? p.pot_rmax : 3.0); }
 
 float g2_threshold(double angle, double lambda)
 {
@@ -150,53 +153,14 @@ Coef coef_for(const ms_params& p, int Z)
 
 void Vr(const Coef& c, double r, double* V, double* dV)
 {
-    double v = 0.0, d = 0.0;
-    switch (c.form) {
-    case MS_POT_DOYLE_0_4:
-    case MS_POT_PENG_0_4:
-    case MS_POT_PENG_0_12: {
-        int n = (c.form == MS_POT_DOYLE_0_4) ? 4 : 5;
-        for (int i = 0; i < n; i++) {
-            double e = c.cl[i] * std::exp(-c.cnl[i] * r * r);
-            v += e;
-            d += -2.0 * c.cnl[i] * r * e;
-        }
-    } break;
-    case MS_POT_KIRKLAND_0_12:
-    case MS_POT_MOLIERE: {
-        for (int i = 0; i < 3; i++) {
-            double e = c.cl[i] * std::exp(-c.cnl[i] * r) / r;
-            v += e;
-            d += -e * (c.cnl[i] + 1.0 / r);
-        }
-        for (int i = 3; i < 6; i++) {
-            double e = c.cl[i] * std::exp(-c.cnl[i] * r * r);
-            v += e;
-            d += -2.0 * c.cnl[i] * r * e;
-        }
-    } break;
-    case MS_POT_WEICKENMEIER_0_12: {
-        double s = 0.0, sd = 0.0;
-        for (int i = 0; i < 6; i++) {
-            s += c.cl[i] * std::erfc(c.cnl[i] * r);
-            sd += c.cl[i] * c.cnl[i] * std::exp(-c.cnl[i] * c.cnl[i] * r * r);
-        }
-        v = s / r;
-        d = -(2.0 * sd / 1.772453850905516027298) / r - s / (r * r);
-    } break;
-    case MS_POT_LOBATO_0_12: {
-        for (int i = 0; i < 5; i++) {
-            double br = c.cnl[i] * r;
-            double e = c.cl[i] * std::exp(-br);
-            v += e * (2.0 / br + 1.0);
-            d += -e * (2.0 / (br * r) + 2.0 / r + c.cnl[i]);
-        }
-    } break;
-    default:
-        break;
+    ElemCoefDev e;
+    e.form = c.form;
+    e.pad = 0;
+    for (int k = 0; k < MS_MAX_COEF; k++) {
+        e.cl[k] = c.cl[k];
+        e.cnl[k] = c.cnl[k];
     }
-    *V = v;
-    *dV = d;
+    vr_eval(e, r, V, dV);
 }
 
 // Projection along z with the substitution z = R sinh(u):
@@ -220,6 +184,42 @@ void project(const Coef& c, double R, double* Vz, double* dVz)
     *dVz = h * sd;
 }
 }  // namespace
+
+ElemCoefDev elem_coef_dev(const ms_params& p, int Z)
+{
+    Coef c = coef_for(p, Z);
+    ElemCoefDev e;
+    e.form = c.form;
+    e.pad = 0;
+    for (int k = 0; k < MS_MAX_COEF; k++) {
+        e.cl[k] = c.cl[k];
+        e.cnl[k] = c.cnl[k];
+    }
+    return e;
+}
+
+void gauss_legendre_half(int n, double* x, double* w)
+{
+    const int m = (n + 1) / 2;
+    for (int i = 0; i < m; i++) {
+        double z = std::cos(kPi * (i + 0.75) / (n + 0.5)), pp = 1.0;
+        for (int it = 0; it < 100; it++) {
+            double p1 = 1.0, p2 = 0.0;
+            for (int j = 1; j <= n; j++) {
+                const double p3 = p2;
+                p2 = p1;
+                p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+            }
+            pp = n * (z * p1 - p2) / (z * z - 1.0);
+            const double z1 = z;
+            z = z1 - p1 / pp;
+            if (std::fabs(z - z1) <= 1e-15) break;
+        }
+        x[i] = -0.5 * z;
+        x[n - 1 - i] = 0.5 * z;
+        w[i] = w[n - 1 - i] = 1.0 / ((1.0 - z * z) * pp * pp);
+    }
+}
 
 void projected_potential_fp64(const ms_params& p, int Z, double R, double* Vz, double* dVz_dR2)
 {
@@ -322,12 +322,18 @@ int host_slices(const ms_params& p, const float* z, int64_t n, std::vector<float
         vmax = std::max(vmax, z[i]);
     }
     float dz = (float)p.dz;
+    const float zmax_atoms = vmax;
+    if (p.enable_fine_slicing) {
+        // planes over the z range grown by the integration radius (slice_generator.hpp:56-76)
+        vmin = MSF_SUB(vmin, fine_radius(p));
+        vmax = MSF_ADD(vmax, fine_radius(p));
+    }
     int nv = det_nplanes(vmin, vmax, dz);
     int border = border_of(p);
     std::vector<float> b(nv);
     for (int i = 0; i < nv; i++) b[i] = det_plane(i, nv, vmin, vmax, dz, border);
     if (atom_slice)
-        for (int64_t k = 0; k < n; k++) atom_slice[k] = det_slice_of(z[k], b.data(), nv, vmax);
+        for (int64_t k = 0; k < n; k++) atom_slice[k] = det_slice_of(z[k], b.data(), nv, zmax_atoms);
     if (bounds) *bounds = b;
     return nv - 1;
 }
@@ -358,7 +364,8 @@ void validate_params(const ms_params& p)
     MS_REQUIRE(p.dz > 0 && std::isfinite(p.dz), MS_ERR_INVALID_ARG, "dz must be positive");
     MS_REQUIRE(p.E0 > 0 && p.E0 < 10000, MS_ERR_INVALID_ARG, "E0 must be in (0, 10000) kV");
     MS_REQUIRE(std::fabs(p.theta) < 1.0, MS_ERR_INVALID_ARG, "beam tilt theta out of range");
-    MS_REQUIRE(p.enable_fine_slicing == 0, MS_ERR_UNSUPPORTED, "fine slicing is not implemented");
+    MS_REQUIRE(p.enable_fine_slicing == 0 || p.enable_fine_slicing == 1, MS_ERR_INVALID_ARG,
+               "enable_fine_slicing must be 0 or 1");
     MS_REQUIRE(p.illumination_model == 0 || (p.illumination_model >= MS_ILLUM_COHERENT && p.illumination_model <= MS_ILLUM_TCC),
                MS_ERR_INVALID_ARG, "illumination_model must be coherent, partial or TCC");
     MS_REQUIRE(p.temporal_spatial_incoh >= 0 && p.temporal_spatial_incoh <= MS_TSI_COHERENT, MS_ERR_INVALID_ARG,

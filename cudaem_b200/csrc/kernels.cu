@@ -17,6 +17,7 @@
 #include "detmath.cuh"
 #include "fft.cuh"
 #include "kernels.cuh"
+#include "vr.cuh"
 
 namespace msb {
 
@@ -917,15 +918,30 @@ __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
 }
 
 
+// the same with the cubic coefficients read from a per-pair table (fine slicing)
+__device__ __forceinline__ float spline_eval_c(const ElemTable& T, const float4* __restrict__ coef, float r2)
+{
+    float lr = __log2f(fmaxf(r2, 1e-30f));
+    int i = __float2int_rd((lr - T.l0) * T.inv_dl);
+    i = min(max(i, 0), MS_NR - 2);
+    if (r2 < T.R2[i]) i = max(i - 1, 0);
+    else if (i < MS_NR - 2 && r2 >= T.R2[i + 1]) i = i + 1;
+    float d = r2 - T.R2[i];
+    const float4 c = __ldg(coef + i);
+    return ((c.w * d + c.z) * d + c.y) * d + c.x;
+}
+
 constexpr int kPotMaxRanges = 64;
 
 __device__ __forceinline__ int floordiv_i(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
 
+template <bool FINE>
 __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
 {
     extern __shared__ __align__(16) unsigned char psm[];
     ElemTable* el = reinterpret_cast<ElemTable*>(psm);
     float4* cand = reinterpret_cast<float4*>(psm + sizeof(ElemTable) * a.n_elem);
+    unsigned* candp = reinterpret_cast<unsigned*>(cand + kPotThreads);   // fine slicing: pair index
     __shared__ int wsum[kPotThreads / 32];
     __shared__ int total_s;
     __shared__ unsigned r_beg[kPotMaxRanges], r_pre[kPotMaxRanges + 1];
@@ -1004,6 +1020,7 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
         for (unsigned vbase = 0; vbase < n_atoms; vbase += kPotThreads) {
             const unsigned v = vbase + t;
             float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
+            unsigned cpi = 0;
             int cnt = 0;
             if (v < n_atoms) {
                 int r = 0;
@@ -1022,6 +1039,7 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
                 const float dyr = fmaxf(0.f, fmaxf(Y0 - ys, ys - Y1));
                 if (dxr * dxr + dyr * dyr < rm * rm) {
                     cv = make_float4(xa, ya, w, __int_as_float(e | ((ox + 4) << 8) | ((oy + 4) << 12)));
+                    cpi = i;
                     cnt = 1;
                 }
             }
@@ -1045,7 +1063,10 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
             }
             __syncthreads();
             const int off = wsum[wid] + incl - cnt;
-            if (cnt > 0) cand[off] = cv;
+            if (cnt > 0) {
+                cand[off] = cv;
+                if (FINE) candp[off] = cpi;
+            }
             __syncthreads();
             const int total = total_s;
             for (int q = 0; q < total; q++) {
@@ -1084,7 +1105,10 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
                         const float r2 = dx2[k] + dy2[r];
-                        if (r2 < rmax2) acc[r][k] += cd.z * spline_eval(T, r2);
+                        if (r2 < rmax2) {
+                            if (FINE) acc[r][k] += cd.z * spline_eval_c(T, a.pair_coef + (size_t)candp[q] * MS_NR, r2);
+                            else acc[r][k] += cd.z * spline_eval(T, r2);
+                        }
                     }
                 }
             }
@@ -1104,8 +1128,14 @@ void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st)
     if (a.nslice <= 0 || n_conf <= 0) return;
     dim3 grid((unsigned)((a.nx / kPotTX) * (a.ny / kPotTY)), (unsigned)a.nslice, (unsigned)n_conf);
     size_t sm = sizeof(ElemTable) * a.n_elem + sizeof(float4) * kPotThreads;
-    cudaFuncSetAttribute(k_potential, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_potential<<<grid, kPotThreads, sm, st>>>(a);
+    if (a.pair_coef) {
+        sm += sizeof(unsigned) * kPotThreads;
+        cudaFuncSetAttribute(k_potential<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_potential<true><<<grid, kPotThreads, sm, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_potential<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_potential<false><<<grid, kPotThreads, sm, st>>>(a);
+    }
     count_launch();
     check_launch("potential");
 }
@@ -1241,6 +1271,150 @@ void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t
                                                               vr_factor, ax, ay, aw, ae);
     count_launch();
     check_launch("gather");
+}
+
+// ---------------------------------------------------------------------------
+// fine slicing: (atom, slice) pairs and their slice-integrated splines
+// (generate_potential_by_height with enable_fine_slicing, projected_potential.cuh:94-133;
+// gen_sa_coeff_kernel and fill_spl_coeff_kernel, device_kernels.cuh:48-105)
+// ---------------------------------------------------------------------------
+__global__ void k_fine_assign(const float* xd, const float* yd, const float* zd, int64_t n, const float* bounds,
+                              int bstride, const int* nv, const float* zmax, int S_cap, CellGrid cg, float rint,
+                              int maxper, unsigned nkeys, unsigned* keys, int* vals, unsigned* counts)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int ci = blockIdx.y;
+    const int64_t o = (int64_t)ci * n + i;
+    const float z = zd[o];
+    const float* b = bounds + (int64_t)ci * bstride;
+    const int ns = nv[ci] - 1;
+    const int ncell = cg.ncx * cg.ncy;
+    const int cell = cell_of(yd[o], cg.ly, cg, cg.ncy) * cg.ncx + cell_of(xd[o], cg.lx, cg, cg.ncx);
+    // candidate slices: every slice whose middle lies within rint + one slice of z (the membership
+    // test below decides exactly)
+    const float dz = b[1] - b[0];
+    int s0 = (int)floorf((z - rint - b[0]) / dz) - 2, s1 = (int)ceilf((z + rint - b[0]) / dz) + 2;
+    s0 = max(s0, 0);
+    s1 = min(s1, ns - 1);
+    int k = 0;
+    for (int s = s0; s <= s1 && k < maxper; s++) {
+        if (!det_fine_member(z, b[s], b[s + 1], rint, zmax[ci])) continue;
+        const unsigned key = ((unsigned)ci * (unsigned)(S_cap + 1) + (unsigned)s) * (unsigned)ncell + (unsigned)cell;
+        keys[o * maxper + k] = key;
+        vals[o * maxper + k] = (int)i;
+        atomicAdd(counts + key, 1u);
+        k++;
+    }
+    for (; k < maxper; k++) {
+        keys[o * maxper + k] = nkeys;
+        vals[o * maxper + k] = (int)i;
+    }
+}
+
+void launch_fine_assign(const float* xd, const float* yd, const float* zd, int64_t n, int nconf, const float* bounds,
+                        int bstride, const int* nv, const float* zmax, int S_cap, const CellGrid& cg, float rint,
+                        int maxper, unsigned nkeys, unsigned* keys, int* vals, unsigned* counts, cudaStream_t st)
+{
+    dim3 grid((unsigned)((n + 255) / 256), (unsigned)nconf);
+    k_fine_assign<<<grid, 256, 0, st>>>(xd, yd, zd, n, bounds, bstride, nv, zmax, S_cap, cg, rint, maxper, nkeys,
+                                        keys, vals, counts);
+    count_launch();
+    check_launch("fine slicing assignment");
+}
+
+__global__ void k_fine_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, CellGrid cg,
+                              unsigned nkeys, const float* xd, const float* yd, const float* zd, const float* occ,
+                              const int* elem, float vr, float* ax, float* ay, float* aw, int* ae, float* az)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const unsigned key = keys[i];
+    if (key >= nkeys) return;   // unused slot (sorted past every pair)
+    const int64_t ci = key / ((unsigned)(S_cap + 1) * (unsigned)(cg.ncx * cg.ncy));
+    const int64_t at = vals[i];
+    const float x = xd[ci * n + at], y = yd[ci * n + at];
+    ax[i] = x;
+    ay[i] = y;
+    az[i] = zd[ci * n + at];
+    aw[i] = vr * occ[at];
+    ae[i] = elem[at] | ((wrap_count(x, cg.lx, cg.wrap) + 8) << 8) | ((wrap_count(y, cg.ly, cg.wrap) + 8) << 12);
+}
+
+void launch_fine_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const CellGrid& cg,
+                        unsigned nkeys, const float* xd, const float* yd, const float* zd, const float* occ,
+                        const int* elem, float vr_factor, float* ax, float* ay, float* aw, int* ae, float* az,
+                        cudaStream_t st)
+{
+    k_fine_gather<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(keys, vals, total, n, S_cap, cg, nkeys, xd, yd, zd,
+                                                                   occ, elem, vr_factor, ax, ay, aw, ae, az);
+    count_launch();
+    check_launch("fine slicing gather");
+}
+
+// One block per pair, one thread per spline node: the atom's potential integrated over the
+// slice by the kNqz-point z quadrature in FP64 (V and dV/dR^2), the cosine taper in R^2 from
+// 0.85 R_max, then the Hermite cubic coefficients of each node interval.
+__global__ void __launch_bounds__(MS_NR) k_fine_tables(const unsigned* keys, const float* az, const int* ae,
+                                                       const unsigned* seg, unsigned nkeys, const float* bounds,
+                                                       int bstride, int S_cap, int ncell, const ElemCoefDev* coefs,
+                                                       double rmin, double rmax, const double* qz, float4* out)
+{
+    const int64_t p = blockIdx.x;
+    if (p >= (int64_t)seg[nkeys]) return;
+    __shared__ double sR2[MS_NR], sV[MS_NR], sdV[MS_NR];
+    const int i = threadIdx.x;
+    const unsigned key = keys[p];
+    const int ci = (int)(key / ((unsigned)(S_cap + 1) * (unsigned)ncell));
+    const int s = (int)((key / (unsigned)ncell) % (unsigned)(S_cap + 1));
+    const float zs = bounds[(int64_t)ci * bstride + s], ze = bounds[(int64_t)ci * bstride + s + 1];
+    const float zm = MSF_MUL(0.5f, MSF_ADD(zs, ze));
+    const double amid = (double)MSF_SUB(zm, az[p]), dzs = (double)MSF_SUB(ze, zs);
+    const ElemCoefDev& c = coefs[ae[p] & 0xFF];
+    const double R = (i == MS_NR - 1) ? rmax : rmin * pow(rmax / rmin, (double)i / (double)(MS_NR - 1));
+    const double R2 = R * R;
+    double v = 0.0, d = 0.0;
+    for (int k = 0; k < kNqz; k++) {
+        const double z = dzs * qz[k] + amid;
+        const double r = sqrt(z * z + R2);
+        double Vr, dVr;
+        vr_eval(c, r, &Vr, &dVr);
+        v += qz[kNqz + k] * dzs * Vr;
+        d += qz[kNqz + k] * dzs * dVr / r;
+    }
+    d *= 0.5;
+    const double R2tap = (0.85 * rmax) * (0.85 * rmax);
+    const double tap_cf = 3.14159265358979323846264338327950288 / (2.0 * (rmax * rmax - R2tap));
+    if (R2tap < R2) {
+        const double tap = cos(tap_cf * (R2 - R2tap)), dtap = sin(tap_cf * (R2 - R2tap));
+        d = d * tap - tap_cf * v * dtap;
+        v = v * tap;
+    }
+    sR2[i] = R2;
+    sV[i] = v;
+    sdV[i] = d;
+    __syncthreads();
+    double c2 = 0.0, c3 = 0.0;
+    if (i < MS_NR - 1) {
+        const double idR = 1.0 / (sR2[i + 1] - R2);
+        const double m = (sV[i + 1] - v) * idR;
+        const double nn = d + sdV[i + 1];
+        c2 = (3.0 * m - nn - d) * idR;
+        c3 = (nn - 2.0 * m) * idR * idR;
+    }
+    out[p * MS_NR + i] = make_float4((float)v, (float)d, (float)c2, (float)c3);
+}
+
+void launch_fine_tables(const unsigned* keys, const float* az, const int* ae, const unsigned* seg, unsigned nkeys,
+                        int64_t total, const float* bounds, int bstride, int S_cap, const CellGrid& cg,
+                        const ElemCoefDev* coefs, double rmin, double rmax, const double* qz, float4* out,
+                        cudaStream_t st)
+{
+    if (total <= 0) return;
+    k_fine_tables<<<(unsigned)total, MS_NR, 0, st>>>(keys, az, ae, seg, nkeys, bounds, bstride, S_cap,
+                                                     cg.ncx * cg.ncy, coefs, rmin, rmax, qz, out);
+    count_launch();
+    check_launch("fine slicing splines");
 }
 
 // ---------------------------------------------------------------------------

@@ -131,7 +131,10 @@ struct PotArgs {
     float rmax_all;             // largest cut-off radius of the elements
     const ElemTable* elems;
     int n_elem;
+    const float4* pair_coef;    // fine slicing: spline coefficients of every sorted (atom, slice) pair
 };
+
+struct ElemCoefDev;
 
 // launchers (kernels.cu); all asynchronous on `st`
 void upload_constants(cudaStream_t st);
@@ -154,6 +157,19 @@ void launch_assign(const float* xd, const float* yd, const float* zd, int64_t n,
 void launch_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const CellGrid& cg,
                    const float* xd, const float* yd, const float* occ, const int* elem, float vr_factor, float* ax,
                    float* ay, float* aw, int* ae, cudaStream_t st);
+// fine slicing: (atom, slice) pairs, maxper slots per atom (unused slots carry the key nkeys),
+// their gather (with the atom's z), and the slice-integrated spline of every pair
+void launch_fine_assign(const float* xd, const float* yd, const float* zd, int64_t n, int nconf, const float* bounds,
+                        int bstride, const int* nv, const float* zmax, int S_cap, const CellGrid& cg, float rint,
+                        int maxper, unsigned nkeys, unsigned* keys, int* vals, unsigned* counts, cudaStream_t st);
+void launch_fine_gather(const unsigned* keys, const int* vals, int64_t total, int64_t n, int S_cap, const CellGrid& cg,
+                        unsigned nkeys, const float* xd, const float* yd, const float* zd, const float* occ,
+                        const int* elem, float vr_factor, float* ax, float* ay, float* aw, int* ae, float* az,
+                        cudaStream_t st);
+void launch_fine_tables(const unsigned* keys, const float* az, const int* ae, const unsigned* seg, unsigned nkeys,
+                        int64_t total, const float* bounds, int bstride, int S_cap, const CellGrid& cg,
+                        const ElemCoefDev* coefs, double rmin, double rmax, const double* qz, float4* out,
+                        cudaStream_t st);
 
 // post-processing
 void launch_detect(const float2* psi, int nwaves, int nx, int ny, float dgx, float dgy, const float* g2in,

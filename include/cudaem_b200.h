@@ -149,7 +149,7 @@ typedef struct ms_params {
     int exec_mode;                /* MS_EXEC_* */
     int probe_batch;              /* probes per batch; 0 lets the autotuner choose */
     int ckpt_interval;            /* adjoint: store the wave every k slices (>= 1) */
-    int enable_fine_slicing;      /* must be 0 */
+    int enable_fine_slicing;      /* 1: per-slice integrated atom potentials (projected_potential.cuh:34-45, :94-133) */
     int gpu_num;                  /* must be 1: one GPU per context */
 } ms_params;
 

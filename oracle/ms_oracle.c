@@ -23,6 +23,7 @@
 #endif
 
 #define OR_PI 3.14159265358979323846264338327950288
+#define MS_NQZ 64 /* z quadrature points of fine slicing (c_nqz) */
 typedef double complex cplx;
 
 static int g_threads = 0;
@@ -151,6 +152,9 @@ void or_displace(const ms_params* p, const ms_atoms* a, int conf, float* x, floa
 /* z_eps is epsilon_rel<float>() of the missing host header, taken as 1e-4    */
 /* (the relative epsilon of the reference's float compare, misc_dev.cuh:17-23)*/
 /* ------------------------------------------------------------------------ */
+static double or_rmin(const ms_params* p) { return p->pot_rmin > 0 ? p->pot_rmin : 0.01; }
+static double or_rmax(const ms_params* p) { return p->pot_rmax > 0 ? p->pot_rmax : 3.0; }
+
 static int or_border(const ms_params* p)
 {
     if (p->slice_border >= 0) return p->slice_border;
@@ -166,6 +170,14 @@ int or_slices(const ms_params* p, const float* z, int64_t n, float* bounds, int 
     for (int64_t i = 1; i < n; i++) {
         if (z[i] < vmin) vmin = z[i];
         if (z[i] > vmax) vmax = z[i];
+    }
+    float zmax_atoms = vmax;
+    if (p->enable_fine_slicing) {
+        /* fine slicing: planes over the atoms' z range grown by the integration radius
+           (get_slice_boundary with atoms.z_int_min/max, slice_generator.hpp:56-76) */
+        const float R_int = (float)or_rmax(p);
+        vmin = vmin - R_int;
+        vmax = vmax + R_int;
     }
     float s_v = vmax - vmin;
     int nv = (int)floorf((s_v + z_eps) / dz) + 2;
@@ -197,7 +209,7 @@ int or_slices(const ms_params* p, const float* z, int64_t n, float* bounds, int 
                     if (b[mid] <= zk) lo = mid; else hi = mid;
                 }
                 s = lo;
-            } else if (zk == b[nv - 1] && zk == vmax) {
+            } else if (zk == b[nv - 1] && zk == zmax_atoms) {
                 s = ns - 1;
             }
             atom_slice[k] = s;
@@ -342,14 +354,113 @@ int or_projected(const ms_params* p, int Z, double R, double* Vz, double* dVz_dR
     return 0;
 }
 
-static double or_rmin(const ms_params* p) { return p->pot_rmin > 0 ? p->pot_rmin : 0.01; }
-static double or_rmax(const ms_params* p) { return p->pot_rmax > 0 ? p->pot_rmax : 3.0; }
 
 /* Radial spline table (the VR_Cubic coefficients of Element_Coeffs,
    device_containers.cuh:243-249): log-spaced nodes in R, values and
    derivatives in R^2, a cosine taper in R^2 from R_tap = 0.85 R_max
    (apply_tapering_dev, basic_functions_dev.cuh:90-101) and Hermite cubic
    coefficients (get_cubic_poly_coef, basic_functions_dev.cuh:76-89). */
+/* R of spline node i: log-spaced from R_min to R_max */
+static double or_node_R(const ms_params* p, int i)
+{
+    double rmn = or_rmin(p), rmx = or_rmax(p);
+    double R = rmn * pow(rmx / rmn, (double)i / (double)(MS_NR - 1));
+    return i == MS_NR - 1 ? rmx : R;
+}
+
+/* Gauss-Legendre nodes and weights on [-1/2, 1/2] with weights summing to 1: the z
+   quadrature qz of fine slicing (gen_sa_coeff_kernel, device_kernels.cuh:48-86; the
+   reference's table comes from the missing multislice_params.hpp).  Newton iteration on the
+   Legendre recurrence from the usual cosine starting points. */
+void or_gauss_legendre_half(int n, double* x, double* w)
+{
+    int m = (n + 1) / 2;
+    for (int i = 0; i < m; i++) {
+        double z = cos(OR_PI * (i + 0.75) / (n + 0.5)), z1, pp = 1.0;
+        for (int it = 0; it < 100; it++) {
+            double p1 = 1.0, p2 = 0.0;
+            for (int j = 1; j <= n; j++) {
+                double p3 = p2;
+                p2 = p1;
+                p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+            }
+            pp = n * (z * p1 - p2) / (z * z - 1.0);
+            z1 = z;
+            z = z1 - p1 / pp;
+            if (fabs(z - z1) <= 1e-15) break;
+        }
+        x[i] = -0.5 * z;
+        x[n - 1 - i] = 0.5 * z;
+        w[i] = w[n - 1 - i] = 1.0 / ((1.0 - z * z) * pp * pp);
+    }
+}
+
+/* Slice-integrated potential of one atom at node R (fine slicing, gen_sa_coeff_kernel,
+   device_kernels.cuh:48-86): V = sum_k w_k dz V(r_k), dV/dR^2 = 1/2 sum_k w_k dz V'(r_k)/r_k,
+   r_k = sqrt(z_k^2 + R^2), z_k = dz x_k + a, a = slice middle - atom z. */
+static void or_fine_node(const or_coef* c, double R, double a, double dzs, double* V, double* dV)
+{
+    double xq[MS_NQZ], wq[MS_NQZ];
+    or_gauss_legendre_half(MS_NQZ, xq, wq);
+    double v = 0.0, d = 0.0;
+    for (int k = 0; k < MS_NQZ; k++) {
+        double z = dzs * xq[k] + a;
+        double r = sqrt(z * z + R * R);
+        double Vr, dVr;
+        or_Vr(c, r, &Vr, &dVr);
+        v += wq[k] * dzs * Vr;
+        d += wq[k] * dzs * dVr / r;
+    }
+    *V = v;
+    *dV = 0.5 * d;
+}
+
+/* taper (apply_tapering_dev, basic_functions_dev.cuh:90-101) and Hermite coefficients
+   (get_cubic_poly_coef, basic_functions_dev.cuh:76-89) of node values c0 and slopes c1 */
+static void or_spline_finish(const ms_params* p, const double* R2, double* c0, double* c1, double* c2, double* c3)
+{
+    double rmx = or_rmax(p);
+    double R2tap = (0.85 * rmx) * (0.85 * rmx);
+    double tap_cf = OR_PI / (2.0 * (rmx * rmx - R2tap));
+    for (int i = 0; i < MS_NR; i++)
+        if (R2tap < R2[i]) {
+            double tap = cos(tap_cf * (R2[i] - R2tap));
+            double dtap = sin(tap_cf * (R2[i] - R2tap));
+            c1[i] = c1[i] * tap - tap_cf * c0[i] * dtap;
+            c0[i] = c0[i] * tap;
+        }
+    for (int i = 0; i < MS_NR - 1; i++) {
+        double idR = 1.0 / (R2[i + 1] - R2[i]);
+        double m = (c0[i + 1] - c0[i]) * idR;
+        double n = c1[i] + c1[i + 1];
+        c2[i] = (3.0 * m - n - c1[i]) * idR;
+        c3[i] = (n - 2.0 * m) * idR * idR;
+    }
+    c2[MS_NR - 1] = 0.0;
+    c3[MS_NR - 1] = 0.0;
+}
+
+/* spline of one (atom, slice) pair under fine slicing */
+static void or_fine_spline(const ms_params* p, int Z, double a, double dzs, double* R2, double* c0, double* c1,
+                           double* c2, double* c3)
+{
+    or_coef c;
+    or_coef_for(p, Z, &c);
+    for (int i = 0; i < MS_NR; i++) {
+        double R = or_node_R(p, i);
+        R2[i] = R * R;
+        or_fine_node(&c, R, a, dzs, &c0[i], &c1[i]);
+    }
+    or_spline_finish(p, R2, c0, c1, c2, c3);
+}
+
+int or_fine_spline_table(const ms_params* p, int Z, double a, double dzs, double* R2, double* c0, double* c1,
+                         double* c2, double* c3)
+{
+    or_fine_spline(p, Z, a, dzs, R2, c0, c1, c2, c3);
+    return 0;
+}
+
 int or_spline(const ms_params* p, int Z, double* R2, double* c0, double* c1, double* c2, double* c3, double* rmax)
 {
     or_coef c;
@@ -357,9 +468,9 @@ int or_spline(const ms_params* p, int Z, double* R2, double* c0, double* c1, dou
     double rmn = or_rmin(p), rmx = or_rmax(p);
     double R2tap = (0.85 * rmx) * (0.85 * rmx);
     double tap_cf = OR_PI / (2.0 * (rmx * rmx - R2tap));
+    (void)rmn;
     for (int i = 0; i < MS_NR; i++) {
-        double R = rmn * pow(rmx / rmn, (double)i / (double)(MS_NR - 1));
-        if (i == MS_NR - 1) R = rmx;
+        double R = or_node_R(p, i);
         double Vz, dVz;
         or_project(&c, R, &Vz, &dVz);
         R2[i] = R * R;
@@ -612,6 +723,37 @@ static int or_spec_build(const ms_params* p, const ms_atoms* a, int conf, or_spe
     sp->bounds = (float*)malloc(sizeof(float) * (size_t)(ns + 1));
     or_slices(p, sp->z, a->n, sp->bounds, ns + 1, sp->slice);
     sp->start = (int64_t*)calloc((size_t)ns + 2, sizeof(int64_t));
+    if (p->enable_fine_slicing) {
+        /* fine slicing: slice i takes every atom with z in its integration range
+           [min(z_m - R, z_start), max(z_m + R, z_end)] grown by z_eps (get_slicing and fd_by_z with
+           Inc_Borders, slice_generator.hpp:78-129): z >= lower and (z < upper, or the highest atom
+           lies at or below upper) */
+        const float z_eps = 1e-4f, R_int = (float)or_rmax(p);
+        float zmax = a->n > 0 ? sp->z[0] : 0.f;
+        for (int64_t i = 1; i < a->n; i++)
+            if (sp->z[i] > zmax) zmax = sp->z[i];
+        int64_t cap = 16, cnt = 0;
+        int64_t* ord = (int64_t*)malloc(sizeof(int64_t) * (size_t)cap);
+        for (int s = 0; s < ns; s++) {
+            float zs = sp->bounds[s], ze = sp->bounds[s + 1];
+            float zm = 0.5f * (zs + ze);
+            float lo = fminf(zm - R_int, zs) - z_eps, hi = fmaxf(zm + R_int, ze) + z_eps;
+            for (int64_t i = 0; i < a->n; i++) {
+                float z = sp->z[i];
+                if (z >= lo && (z < hi || zmax <= hi)) {
+                    if (cnt == cap) {
+                        cap *= 2;
+                        ord = (int64_t*)realloc(ord, sizeof(int64_t) * (size_t)cap);
+                    }
+                    ord[cnt++] = i;
+                }
+            }
+            sp->start[s + 1] = cnt;
+        }
+        sp->order = ord;
+        sp->z_init = ns > 0 ? (double)(float)(0.5 * (double)(sp->bounds[1] + sp->bounds[0])) : 0.0;
+        return ns;
+    }
     sp->order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(a->n + 1));
     for (int64_t i = 0; i < a->n; i++)
         if (sp->slice[i] >= 0) sp->start[sp->slice[i] + 1]++;
@@ -667,9 +809,21 @@ static void or_slice_potential(const ms_params* p, const ms_atoms* a, const or_s
 {
     memset(V, 0, sizeof(double) * (size_t)s->N);
     if (islice < 0 || islice >= sp->ns) return;
+    or_elem fe;
     for (int64_t k = sp->start[islice]; k < sp->start[islice + 1]; k++) {
         int64_t ia = sp->order[k];
         or_elem* e = or_elem_get(p, es, a->Z[ia]);
+        if (p->enable_fine_slicing) {
+            /* the atom's potential integrated over this slice (generate_potential_by_height with
+               z_middle = slice middle - atom z, projected_potential.cuh:94-133) */
+            float zs = sp->bounds[islice], ze = sp->bounds[islice + 1];
+            float zm = 0.5f * (ze + zs);
+            double a_mid = (double)(zm - sp->z[ia]);
+            or_fine_spline(p, a->Z[ia], a_mid, (double)(ze - zs), fe.R2, fe.c0, fe.c1, fe.c2, fe.c3);
+            fe.rmax = e->rmax;
+            fe.Z = e->Z;
+            e = &fe;
+        }
         double xa = sp->x[ia], ya = sp->y[ia];
         double rmax2 = e->rmax * e->rmax;
         double coeff = s->vr_factor * (double)a->occ[ia];
@@ -886,7 +1040,7 @@ static double or_pctf_env(const ms_params* p, double lambda, double g2)
 /* the image-forming lens on an exit wave in reciprocal space: apply_CTF_kernel (device_kernels.cuh:
    445-468) with the frequency shift (gxu, gyu), the optional envelope, and an amplitude factor;
    then the inverse FFT.  out may be W itself (the update is element by element). */
-static void or_ctf_image(const ms_params* p, const or_sim* s, const or_lens* L, double gxu, double gyu, int pctf,
+static void or_ctf_apply(const ms_params* p, const or_sim* s, const or_lens* L, double gxu, double gyu, int pctf,
                          double amp, const cplx* W, cplx* out)
 {
     float gxuf = (float)gxu, gyuf = (float)gyu;
@@ -905,6 +1059,12 @@ static void or_ctf_image(const ms_params* p, const or_sim* s, const or_lens* L, 
             } else
                 out[k] = 0.0;
         }
+}
+
+static void or_ctf_image(const ms_params* p, const or_sim* s, const or_lens* L, double gxu, double gyu, int pctf,
+                         double amp, const cplx* W, cplx* out)
+{
+    or_ctf_apply(p, s, L, gxu, gyu, pctf, amp, W, out);
     or_fft2c(out, s->nx, s->ny, +1);
 }
 
@@ -1287,5 +1447,85 @@ int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_
     *dL_dC30 = g30;
     free(T);
     free(P);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* operator-level entry points, checked against the reference's own kernels  */
+/* (oracle/ref_shim) on the same inputs                                      */
+/* ------------------------------------------------------------------------ */
+int or_op_propagator(const ms_params* p, double* P)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    or_propagator(p, &s, (cplx*)P);
+    return 0;
+}
+
+int or_op_probe(const ms_params* p, double px, double py, double z_init, double* W)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    or_lens L;
+    or_lens_init(&p->cond_lens, s.lambda, z_init, &L);
+    or_probe_k(&s, &L, px, py, (cplx*)W);
+    return 0;
+}
+
+int or_op_ctf(const ms_params* p, int pctf, double c10_shift, double gxu, double gyu, const double* in, double* out)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    or_lens L;
+    or_lens_init(&p->obj_lens, s.lambda, c10_shift, &L);
+    or_ctf_apply(p, &s, &L, gxu, gyu, pctf, 1.0, (const cplx*)in, (cplx*)out);
+    return 0;
+}
+
+int or_op_detect(const ms_params* p, const double* W, double* Iout)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    or_detect(p, &s, (const cplx*)W, Iout);
+    return 0;
+}
+
+int or_op_slice_potential(const ms_params* p, int Z, int64_t n, const float* x, const float* y, const float* occ,
+                          double* V)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    or_spec sp;
+    memset(&sp, 0, sizeof(sp));
+    int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+    int64_t start[2] = {0, n};
+    int* Zs = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int64_t i = 0; i < n; i++) {
+        order[i] = i;
+        Zs[i] = Z;
+    }
+    float* xx = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* yy = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    memcpy(xx, x, sizeof(float) * (size_t)n);
+    memcpy(yy, y, sizeof(float) * (size_t)n);
+    ms_atoms a;
+    memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.Z = Zs;
+    a.x = x;
+    a.y = y;
+    a.occ = occ;
+    sp.ns = 1;
+    sp.start = start;
+    sp.order = order;
+    sp.x = xx;
+    sp.y = yy;
+    or_slice_potential(p, &a, &s, &sp, es, 0, V);
+    free(order);
+    free(Zs);
+    free(xx);
+    free(yy);
+    free(es);
     return 0;
 }

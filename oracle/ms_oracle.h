@@ -7,12 +7,14 @@
  * of bench.py use it.
  *
  * Parity status: the reference publishes no golden vectors and its source
- * cannot be built as shipped (eleven headers are missing), so agreement
- * with the reference's own outputs is pinned only through the
- * reference-kernel shim under oracle/ref_shim/ (the reference's device
- * kernels compiled with a small constants header) where that run exists;
- * otherwise parity with the reference is unpinned and rests on the
- * file:line restatement below plus physics invariants.
+ * cannot be built as shipped (eleven headers are missing).  Its device
+ * kernels do compile from their own files with the small constants header
+ * in oracle/ref_shim/, so each per-pixel operator below (propagator, probe,
+ * CTF and PCTF, detector sum, spline potential) is pinned against the
+ * reference's own kernels on the same inputs (or_op_* entry points); the
+ * host-side pieces whose sources are missing (slicing driver, phonon RNG,
+ * quadrature tables, element tables) and the composed simulations rest on
+ * the file:line restatement plus physics invariants.
  */
 #ifndef MS_ORACLE_H
 #define MS_ORACLE_H
@@ -60,6 +62,22 @@ int or_stem_forward_potential(const ms_params* p, const float* V, int n_slices, 
 int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_init,
                      const double* probe_xy, int n_probe, const float* target, double* loss,
                      double* dL_dV, double* dL_dC10, double* dL_dC30);
+
+/* operator-level entry points, checked against the reference's own kernels (ref_shim/):
+   propagator table, k-space probe, CTF / PCTF (no inverse FFT), detector sums, and the slice
+   potential of atoms of one element; complex arrays interleaved re, im */
+int or_op_propagator(const ms_params* p, double* P);
+int or_op_probe(const ms_params* p, double px, double py, double z_init, double* W);
+int or_op_ctf(const ms_params* p, int pctf, double c10_shift, double gxu, double gyu, const double* in, double* out);
+int or_op_detect(const ms_params* p, const double* W, double* Iout);
+int or_op_slice_potential(const ms_params* p, int Z, int64_t n, const float* x, const float* y, const float* occ,
+                          double* V);
+
+/* fine slicing: Gauss-Legendre quadrature on [-1/2, 1/2] (weights sum to 1) and the spline of
+   one atom's potential integrated over a slice of thickness dzs whose middle lies a above it */
+void or_gauss_legendre_half(int n, double* x, double* w);
+int or_fine_spline_table(const ms_params* p, int Z, double a, double dzs, double* R2, double* c0, double* c1,
+                         double* c2, double* c3);
 
 /* Gauss-Hermite quadrature for exp(-x^2), weights normalised to sum 1 */
 void or_gauss_hermite(int n, double* x, double* w);

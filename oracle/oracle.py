@@ -18,9 +18,40 @@ LIB_PATH = os.path.join(HERE, "_build", "libmsoracle.so")
 _LIB = None
 
 
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libref_kernels.so")
+REF_TREE = "/root/reference"
+
+
 def build() -> str:
     subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    if os.path.isdir(REF_TREE):
+        # the reference's own kernels: built only where the reference tree exists
+        subprocess.run(["make", "-C", HERE, "-s", "ref", f"REF={REF_TREE}"], check=True)
     return LIB_PATH
+
+
+_REF = None
+
+
+def ref_lib():
+    """The reference-kernel shim (oracle/_ref/libref_kernels.so), or None when it was not built."""
+    global _REF
+    if _REF is None and os.path.exists(REF_LIB_PATH):
+        L = C.CDLL(REF_LIB_PATH)
+        P, f, d, i = C.POINTER, C.c_float, C.c_double, C.c_int
+        sig = {
+            "ref_propagator": [i, i, d, d, d, i, d, P(f)],
+            "ref_probe": [i, i, d, d, d, d, d, f, f, d, d, P(f)],
+            "ref_ctf": [i, i, d, d, d, d, d, f, f, i, d, d, d, d, P(f), P(f)],
+            "ref_detector": [i, i, d, d, f, f, P(f), P(d)],
+            "ref_potential": [i, i, d, d, i, P(f), P(f), P(f), P(f), P(f), P(f), P(f), P(f), d, d, P(f)],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.restype = i
+            fn.argtypes = args
+        _REF = L
+    return _REF
 
 
 def lib() -> C.CDLL:
@@ -50,6 +81,13 @@ def lib() -> C.CDLL:
             "or_stem_forward_potential": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(d)]),
             "or_stem_backward": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(f), P(d), P(d), P(d), P(d)]),
             "or_gauss_hermite": (None, [i, P(d), P(d)]),
+            "or_gauss_legendre_half": (None, [i, P(d), P(d)]),
+            "or_fine_spline_table": (i, [P(abi.ms_params), i, d, d, P(d), P(d), P(d), P(d), P(d)]),
+            "or_op_propagator": (i, [P(abi.ms_params), P(d)]),
+            "or_op_probe": (i, [P(abi.ms_params), d, d, d, P(d)]),
+            "or_op_ctf": (i, [P(abi.ms_params), i, d, d, d, P(d), P(d)]),
+            "or_op_detect": (i, [P(abi.ms_params), P(d), P(d)]),
+            "or_op_slice_potential": (i, [P(abi.ms_params), i, C.c_int64, P(f), P(f), P(f), P(d)]),
             "or_set_threads": (None, [i]),
             "or_get_threads": (i, []),
         }

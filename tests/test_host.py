@@ -46,15 +46,20 @@ def test_phonon_axes_flags():
 
 @pytest.mark.parametrize("border", [-1, 0, 1, 2])
 @pytest.mark.parametrize("conf", [0, 3])
-def test_slicing_bit_identical_to_oracle(border, conf):
+@pytest.mark.parametrize("fine", [0, 1])
+def test_slicing_bit_identical_to_oracle(border, conf, fine):
     p, at = cases.hrtem_small(cells=(3, 3, 6), nconf=4)
     p.slice_border = border
+    p.enable_fine_slicing = fine
     b, s = cb.build_slices(p, at, conf)
     _, _, z = orc.displace(p, at, conf)
     bo, so = orc.slices(p, z)
     assert np.array_equal(b, bo) and np.array_equal(s, so)
     assert np.all(np.diff(b) > 0)
-    assert s.min() >= 0 and s.max() == b.size - 2
+    if fine:   # the planes extend one integration radius beyond the atoms on either side
+        assert s.min() > 0 and s.max() < b.size - 2
+    else:
+        assert s.min() >= 0 and s.max() == b.size - 2
 
 
 @pytest.mark.parametrize("name,expected", [("hrtem", 40), ("cbed", 240), ("stem", 50), ("adjoint", 80)])
@@ -85,7 +90,7 @@ def test_crystal_builder():
 
 @pytest.mark.parametrize("field,value,status", [
     ("nx", 100, abi.MS_ERR_UNSUPPORTED), ("ny", 4096, abi.MS_ERR_UNSUPPORTED), ("dz", 0.0, abi.MS_ERR_INVALID_ARG),
-    ("E0", -1.0, abi.MS_ERR_INVALID_ARG), ("enable_fine_slicing", 1, abi.MS_ERR_UNSUPPORTED),
+    ("E0", -1.0, abi.MS_ERR_INVALID_ARG), ("enable_fine_slicing", 2, abi.MS_ERR_INVALID_ARG),
     ("illumination_model", 9, abi.MS_ERR_INVALID_ARG), ("temporal_spatial_incoh", 7, abi.MS_ERR_INVALID_ARG),
     ("gpu_num", 2, abi.MS_ERR_UNSUPPORTED),
     ("n_det", 9, abi.MS_ERR_INVALID_ARG), ("phonon_model", 2, abi.MS_ERR_INVALID_ARG),

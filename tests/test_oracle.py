@@ -179,3 +179,36 @@ def test_gauss_hermite_known_answers():
         assert abs(np.dot(w, x ** 4) - 0.75) < 1e-11
         assert abs(np.dot(w, x ** 6) - 15 / 8) < 1e-10
         assert abs(np.dot(w, x ** 3)) < 1e-12
+
+
+def test_fine_slicing_integrates_the_projection():
+    """Fine slicing splits an atom's potential over the slices whose integration range reaches it:
+    the slice-integrated splines (64-point Gauss-Legendre in z) of all those slices add up to
+    the projected spline wherever the integrand is smooth on the slice scale (R >= 0.1 A), up to
+    the potential's tail beyond the integration radius (R_max = 6 A here: about 1e-3 absolute for
+    Si, 3e-4 relative at R = 2 A)."""
+    import ctypes as C
+    p, _ = cases.cbed_small()
+    p.pot_rmax = 6.0
+    L = orc.lib()
+    d = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    R2, c0 = np.empty(128), np.empty(128)
+    tmp = [np.empty(128) for _ in range(3)]
+    L.or_spline(C.byref(p.c()), 14, d(R2), d(c0), d(tmp[0]), d(tmp[1]), d(tmp[2]), C.byref(C.c_double()))
+    dz, za, rint = 1.358, 0.3, 6.0
+    tot = np.zeros(128)
+    for s in range(-8, 9):
+        zs, ze = s * dz, (s + 1) * dz
+        zm = 0.5 * (zs + ze)
+        if not (min(zm - rint, zs) <= za < max(zm + rint, ze)):
+            continue
+        f = [np.empty(128) for _ in range(5)]
+        L.or_fine_spline_table(C.byref(p.c()), 14, zm - za, dz, *(d(x) for x in f))
+        tot += f[1]
+    R = np.sqrt(R2)
+    sel = (R >= 0.1) & (R <= 2.0)
+    assert np.max(np.abs(tot[sel] - c0[sel]) / np.abs(c0[sel])) < 4e-4
+    assert np.max(np.abs(tot[sel] - c0[sel])) < 2e-3
+    x, w = np.empty(64), np.empty(64)
+    L.or_gauss_legendre_half(64, d(x), d(w))
+    assert abs(w.sum() - 1) < 1e-13 and abs(np.dot(w, x ** 2) - 1 / 12) < 1e-14 and abs(np.dot(w, x ** 4) - 1 / 80) < 1e-14
