@@ -1372,14 +1372,15 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
     const int nseg = (S + k - 1) / k;
     // probes per batch: adjoint wave, forward wave, one segment of transmitted waves and the
     // checkpoints must fit the memory budget
-    const size_t per_wave = (size_t)N * 8 * (2 + (size_t)k + (size_t)(nseg - 1));
+    const size_t per_wave = (size_t)N * 8 * (2 + 2 * (size_t)k + (size_t)(nseg - 1));
     int B = p.probe_batch > 0 ? p.probe_batch : 256;
     B = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, free_budget() / per_wave));
     B = std::min(B, np);
     const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
     const int tiles = col_tiles(p.ny, p.nx);
     float2* adj = (float2*)c->buf("adj_psi", sizeof(float2) * N * B);
-    float2* xseg = (float2*)c->buf("adj_xseg", sizeof(float2) * N * B * k);
+    // transmitted waves of two segments: the one being swept back and the one being recomputed
+    float2* xseg = (float2*)c->buf("adj_xseg", sizeof(float2) * N * B * k * 2);
     float2* ckpt = nseg > 1 ? (float2*)c->buf("adj_ckpt", sizeof(float2) * N * B * (nseg - 1)) : nullptr;
     float* gV = on_dev ? dV : (float*)c->buf("adj_dV", sizeof(float) * slot);
     double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
@@ -1415,13 +1416,14 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
         pa.tw = s.tw_y;
         run_col(c, p.ny, COL_PROBE_INV, pa, nb, p.nx, st);
         const int last0 = (nseg - 1) * k;
+        auto xbuf = [&](int seg) { return xseg + (int64_t)(seg % 2) * k * wstride; };
         for (int sl = 0; sl < S; sl++) {
             if (sl < last0 && sl % k == 0)
                 CK(cudaMemcpyAsync(ckpt + (int64_t)(sl / k) * wstride, adj, sizeof(float2) * wstride,
                                    cudaMemcpyDeviceToDevice, st));
             pa.slice = sl;
             pa.flags = sl >= last0 ? PF_STORE_X : 0;
-            pa.xs = xseg + (int64_t)(sl - last0) * wstride;
+            pa.xs = xbuf(nseg - 1) + (int64_t)(sl - last0) * wstride;
             pa.tw = s.tw_x;
             run_row(c, p.nx, ROW_INV_T_FWD, pa, nb, p.ny, st);
             pa.flags = 0;
@@ -1433,29 +1435,48 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
         launch_resid(Iw, dtgt + (int64_t)start * ndet, nb * ndet, resid, sq + (int64_t)start * ndet, st);
         pa.tw = s.tw_y;
         run_col(c, p.ny, COL_SEED, pa, nb, p.nx, st);
+        // Segments are recomputed on a second stream one segment ahead of the backward sweep,
+        // into the other half of the transmitted-wave buffer; events order each recompute after
+        // the sweep that last read its half, and each sweep after its recompute.  With
+        // per-launch profiling on, everything runs in order on the context stream.
+        const bool two = !c->profile && nseg > 1;
+        cudaStream_t rs = two ? pot_stream(c) : st;
+        auto recompute = [&](int seg) {
+            const int c0 = seg * k, c1 = std::min(S, c0 + k);
+            PassArgs pr = pa;
+            pr.psi = ckpt + (int64_t)seg * wstride;   // in place on the segment's checkpoint
+            for (int sl = c0; sl < c1; sl++) {
+                pr.slice = sl;
+                pr.flags = PF_STORE_X;
+                pr.xs = xbuf(seg) + (int64_t)(sl - c0) * wstride;
+                pr.tw = s.tw_x;
+                run_row(c, p.nx, ROW_INV_T_FWD, pr, nb, p.ny, rs);
+                if (sl < c1 - 1) {
+                    pr.flags = 0;
+                    pr.tw = s.tw_y;
+                    run_col(c, p.ny, COL_STEP, pr, nb, p.nx, rs);
+                }
+            }
+        };
+        auto ev_rec = [&](int seg) { return chunk_event(c, (size_t)(2 * seg)); };
+        auto ev_back = [&](int seg) { return chunk_event(c, (size_t)(2 * seg + 1)); };
+        if (two) {
+            cudaEvent_t fwd_done = chunk_event(c, (size_t)(2 * nseg));
+            CK(cudaEventRecord(fwd_done, st));
+            CK(cudaStreamWaitEvent(rs, fwd_done, 0));
+            recompute(nseg - 2);
+            CK(cudaEventRecord(ev_rec(nseg - 2), rs));
+        }
         for (int seg = nseg - 1; seg >= 0; seg--) {
             const int c0 = seg * k, c1 = std::min(S, c0 + k);
             if (seg != nseg - 1) {
-                // recompute the segment's transmitted waves in place on its checkpoint
-                PassArgs pr = pa;
-                pr.psi = ckpt + (int64_t)seg * wstride;
-                for (int sl = c0; sl < c1; sl++) {
-                    pr.slice = sl;
-                    pr.flags = PF_STORE_X;
-                    pr.xs = xseg + (int64_t)(sl - c0) * wstride;
-                    pr.tw = s.tw_x;
-                    run_row(c, p.nx, ROW_INV_T_FWD, pr, nb, p.ny, st);
-                    if (sl < c1 - 1) {
-                        pr.flags = 0;
-                        pr.tw = s.tw_y;
-                        run_col(c, p.ny, COL_STEP, pr, nb, p.nx, st);
-                    }
-                }
+                if (two) CK(cudaStreamWaitEvent(st, ev_rec(seg), 0));
+                else recompute(seg);
             }
             for (int i = c1 - 1; i >= c0; i--) {
                 pa.slice = i;
                 pa.flags = 0;
-                pa.xs = xseg + (int64_t)(i - c0) * wstride;
+                pa.xs = xbuf(seg) + (int64_t)(i - c0) * wstride;
                 pa.dV = gV + (int64_t)i * N;
                 pa.tw = s.tw_x;
                 run_row(c, p.nx, ROW_ADJ, pa, nb, p.ny, st);
@@ -1468,6 +1489,13 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
                     run_col(c, p.ny, COL_GRAD_PROBE, pa, nb, p.nx, st);
                     launch_chi_finalize(chi_part, nb, tiles, chi_acc, st);
                 }
+            }
+            if (two && seg - 2 >= 0) {
+                // the segment two below reuses this segment's half of the buffer
+                CK(cudaEventRecord(ev_back(seg), st));
+                CK(cudaStreamWaitEvent(rs, ev_back(seg), 0));
+                recompute(seg - 2);
+                CK(cudaEventRecord(ev_rec(seg - 2), rs));
             }
         }
         CK(cudaStreamSynchronize(st));  // the host wave table is refilled by the next batch

@@ -12,6 +12,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <set>
+#include <tuple>
 #include <cfloat>
 
 #include "detmath.cuh"
@@ -26,6 +29,27 @@ int64_t kernel_launches() { return g_launches.load(); }
 void reset_kernel_launches() { g_launches.store(0); }
 void add_kernel_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// Raises a kernel's dynamic shared-memory limit once per device and size (the attribute stays
+// set for the process) instead of before every launch: the slice loop launches thousands of
+// kernels per call and the host must keep ahead of them.
+static std::mutex g_attr_mtx;
+static std::set<std::tuple<int, const void*, size_t>> g_attr_done;
+
+template <class F>
+static void smem_attr(F* kernel, size_t bytes)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, (const void*)kernel, bytes);
+    {
+        std::lock_guard<std::mutex> lk(g_attr_mtx);
+        if (g_attr_done.count(key)) return;
+    }
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    std::lock_guard<std::mutex> lk(g_attr_mtx);
+    g_attr_done.insert(key);
+}
 
 static void check_launch(const char* what)
 {
@@ -656,7 +680,7 @@ static bool row_pipe(const PassArgs& a, int nwaves, int ny, cudaStream_t st)
         const int64_t blocks = std::min<int64_t>((items + 7) / 8, num_sms());
         const size_t sm = sizeof(float2) * ((size_t)(kPipeThreads / 32) * R * L::SCR_STRIDE_ROW + 2 * N + kExpTab) +
                           sizeof(float) * (size_t)(kPipeThreads / 32) * 2 * R * N;
-        cudaFuncSetAttribute(k_row_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row_p<N>, sm);
         k_row_p<N><<<(unsigned)blocks, kPipeThreads, sm, st>>>(a, nwaves);
         return true;
     }
@@ -672,7 +696,7 @@ static bool col_pipe(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
         const int64_t items = (int64_t)nwaves * (nx / L::TC);
         const int64_t blocks = std::min<int64_t>(items, num_sms());
         const size_t sm = sizeof(float2) * ((size_t)L::TC * L::SCR_STRIDE_COL + 2 * N + (size_t)N * L::TC);
-        cudaFuncSetAttribute(k_col_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col_p<N>, sm);
         k_col_p<N><<<(unsigned)blocks, kPipeThreads, sm, st>>>(a, nwaves);
         return true;
     }
@@ -691,27 +715,27 @@ static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStre
     if (op == ROW_INV_T_FWD && (a.flags & PF_STORE_X)) op = ROW_INV_T_FWD_X;
     switch (op) {
     case ROW_T_FWD:
-        cudaFuncSetAttribute(k_row<N, ROW_T_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row<N, ROW_T_FWD>, sm);
         k_row<N, ROW_T_FWD><<<grid, block, sm, st>>>(a);
         break;
     case ROW_INV_T_FWD:
-        cudaFuncSetAttribute(k_row<N, ROW_INV_T_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row<N, ROW_INV_T_FWD>, sm);
         k_row<N, ROW_INV_T_FWD><<<grid, block, sm, st>>>(a);
         break;
     case ROW_INV_ABS2:
-        cudaFuncSetAttribute(k_row<N, ROW_INV_ABS2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row<N, ROW_INV_ABS2>, sm);
         k_row<N, ROW_INV_ABS2><<<grid, block, sm, st>>>(a);
         break;
     case ROW_INV_STORE:
-        cudaFuncSetAttribute(k_row<N, ROW_INV_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row<N, ROW_INV_STORE>, sm);
         k_row<N, ROW_INV_STORE><<<grid, block, sm, st>>>(a);
         break;
     case ROW_ADJ:
-        cudaFuncSetAttribute(k_row<N, ROW_ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row<N, ROW_ADJ>, sm);
         k_row<N, ROW_ADJ><<<grid, block, sm, st>>>(a);
         break;
     case ROW_INV_T_FWD_X:
-        cudaFuncSetAttribute(k_row<N, ROW_INV_T_FWD_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_row<N, ROW_INV_T_FWD_X>, sm);
         k_row<N, ROW_INV_T_FWD_X><<<grid, block, sm, st>>>(a);
         break;
     default: throw MsError(MS_ERR_INTERNAL, "unknown row pass");
@@ -729,31 +753,31 @@ static void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStre
     size_t sm = L::COL_SMEM;
     switch (op) {
     case COL_PROBE_INV:
-        cudaFuncSetAttribute(k_col<N, COL_PROBE_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_PROBE_INV>, sm);
         k_col<N, COL_PROBE_INV><<<grid, block, sm, st>>>(a);
         break;
     case COL_STEP:
-        cudaFuncSetAttribute(k_col<N, COL_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_STEP>, sm);
         k_col<N, COL_STEP><<<grid, block, sm, st>>>(a);
         break;
     case COL_INV:
-        cudaFuncSetAttribute(k_col<N, COL_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_INV>, sm);
         k_col<N, COL_INV><<<grid, block, sm, st>>>(a);
         break;
     case COL_CTF_INV:
-        cudaFuncSetAttribute(k_col<N, COL_CTF_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_CTF_INV>, sm);
         k_col<N, COL_CTF_INV><<<grid, block, sm, st>>>(a);
         break;
     case COL_STEP_SEP:
-        cudaFuncSetAttribute(k_col<N, COL_STEP_SEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_STEP_SEP>, sm);
         k_col<N, COL_STEP_SEP><<<grid, block, sm, st>>>(a);
         break;
     case COL_SEED:
-        cudaFuncSetAttribute(k_col<N, COL_SEED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_SEED>, sm);
         k_col<N, COL_SEED><<<grid, block, sm, st>>>(a);
         break;
     case COL_GRAD_PROBE:
-        cudaFuncSetAttribute(k_col<N, COL_GRAD_PROBE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_col<N, COL_GRAD_PROBE>, sm);
         k_col<N, COL_GRAD_PROBE><<<grid, block, sm, st>>>(a);
         break;
     default: throw MsError(MS_ERR_INTERNAL, "unknown column pass");
@@ -906,12 +930,13 @@ constexpr int kPotRowsPerThread = kPotTY / (kPotThreads / (kPotTX / 4));   // 2 
 __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
 {
     // index of unrolledBinarySearch_c_nR (basic_functions_dev.cuh:47-67): the largest node
-    // i <= nR-2 with R2[i] <= r2 (or 0), from a log2 guess corrected by one comparison
+    // i <= nR-2 with R2[i] <= r2 (or 0).  The nodes are log-spaced, so the index is the floor of
+    // log2(r2) on the node scale; a guess off by one (r2 within the log2 rounding, ~1e-6, of a
+    // node) evaluates the neighbouring cubic a hair outside its interval, which the Hermite
+    // spline's continuity of value and slope makes equal to 1e-12.
     float lr = __log2f(fmaxf(r2, 1e-30f));
     int i = __float2int_rd((lr - T.l0) * T.inv_dl);
     i = min(max(i, 0), MS_NR - 2);
-    if (r2 < T.R2[i]) i = max(i - 1, 0);
-    else if (i < MS_NR - 2 && r2 >= T.R2[i + 1]) i = i + 1;
     float d = r2 - T.R2[i];
     const ElemCoef4 c = T.c[i];
     return ((c.c3 * d + c.c2) * d + c.c1) * d + c.c0;  // get_value_Cubic_Spline
@@ -924,8 +949,6 @@ __device__ __forceinline__ float spline_eval_c(const ElemTable& T, const float4*
     float lr = __log2f(fmaxf(r2, 1e-30f));
     int i = __float2int_rd((lr - T.l0) * T.inv_dl);
     i = min(max(i, 0), MS_NR - 2);
-    if (r2 < T.R2[i]) i = max(i - 1, 0);
-    else if (i < MS_NR - 2 && r2 >= T.R2[i + 1]) i = i + 1;
     float d = r2 - T.R2[i];
     const float4 c = __ldg(coef + i);
     return ((c.w * d + c.z) * d + c.y) * d + c.x;
@@ -1130,10 +1153,10 @@ void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st)
     size_t sm = sizeof(ElemTable) * a.n_elem + sizeof(float4) * kPotThreads;
     if (a.pair_coef) {
         sm += sizeof(unsigned) * kPotThreads;
-        cudaFuncSetAttribute(k_potential<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_potential<true>, sm);
         k_potential<true><<<grid, kPotThreads, sm, st>>>(a);
     } else {
-        cudaFuncSetAttribute(k_potential<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_attr(k_potential<false>, sm);
         k_potential<false><<<grid, kPotThreads, sm, st>>>(a);
     }
     count_launch();
