@@ -60,9 +60,10 @@ def parse():
 def workload(config: str, rank: int = 0, cells_z: int = 0, nconf: int = 0):
     from cudaem_b200 import workloads as wl
     if config == "cbed":
+        from cudaem_b200 import replicas
         cz = cells_z or 60
         p, at = wl.cbed_si(cells=(16, 16, cz), nconf=nconf or 8)
-        p.pn_seed = 42 + 1000 * rank
+        p = replicas.for_rank(p, rank)   # each rank its own phonon configurations
         units = p.pn_nconf * 4 * cz
         desc = {"workload": "CBED Si[001] 16x16x60 cells, 1024^2, 240 slices x 1.358 A, 300 kV, 20 mrad, "
                             "8 frozen-phonon configurations per call", "grid": 1024, "slices": 240,
@@ -335,10 +336,11 @@ def run_ours(args):
     co.on_device = 1
     fn = {"cbed": L.ms_simulate_cbed, "stem": L.ms_simulate_stem, "hrtem": L.ms_simulate_tem}[args.config]
 
+    from cudaem_b200 import replicas
+
     def step(o):
         ctx.check(fn(ctx.handle, C.byref(cp), C.byref(ca), C.byref(o)))
-        if dist is not None:
-            dist.all_reduce(out_dev)
+        replicas.sum_patterns(out_dev, dist)
 
     for _ in range(args.warmup):
         step(co)
@@ -357,11 +359,7 @@ def run_ours(args):
             launches += ctx.last_launch_count
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda", dist=dist)
     value = units * world * args.steps / (ms / 1e3)
 
     # end to end: host atoms in, host pattern out, wall clock around the public call
@@ -377,11 +375,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         ctx.check(fn(ctx.handle, C.byref(cp), C.byref(ca), C.byref(ch)))
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda", dist=dist)
     e2e = units * world * args.steps / e2e_s
     h2d = at.n * (4 * 6)
     d2h = host_out.nbytes

@@ -558,6 +558,7 @@ PotArgs pot_args(const ms_params& p, const Setup& s, const AtomsDev& A, const Sp
                  int64_t conf_stride, int slice0, int nslice, int base)
 {
     PotArgs a;
+    std::memset(&a, 0, sizeof(a));
     a.ax = g.ax; a.ay = g.ay; a.aw = g.aw; a.ae = g.ae; a.seg = g.seg; a.ns = g.ns_d;
     a.S_cap = g.S_cap;
     a.slice0 = slice0;
@@ -640,6 +641,16 @@ PotChunks launch_potential_chunks(ms_ctx* c, PotArgs a, int n_conf, int S)
         CK(cudaEventRecord(pc.ev[k], side));
     }
     return pc;
+}
+
+// The potential kernel writing the transmission function t = exp(i V) (complex) instead of V:
+// the slice passes then read t, and the exponential is formed once per pixel and slice, on the
+// potential kernel's side stream, instead of in the latency-bound row pass.
+PotArgs with_transmission(PotArgs a, float2* T, const Setup& s)
+{
+    a.T = T;
+    a.exptab = s.exptab;
+    return a;
 }
 
 PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const float* sV, int64_t slot_stride,
@@ -748,7 +759,7 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
 
     // configurations per group: potential store + waves must fit the memory budget
     int S_est = estimate_slices(p, a);
-    size_t per_conf = (size_t)S_est * N * 4 + (size_t)N * 8 * 2 + (size_t)N * 4 + (size_t)a.n * 40 +
+    size_t per_conf = (size_t)S_est * N * 8 + (size_t)N * 8 * 2 + (size_t)N * 4 + (size_t)a.n * 40 +
                       fine_bytes_per_conf(p, a);
     int gsize = (int)std::max<size_t>(1, std::min<size_t>(cs.confs.size(), free_budget() / per_conf));
 
@@ -762,12 +773,14 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         if (g0 == 0) ns_first = g.ns[0];
         const int nw = g.nconf;
         const int64_t slot = (int64_t)g.S_cap * N;
-        float* sV = (float*)c->buf("sV", sizeof(float) * slot * nw);
+        float2* sT = (float2*)c->buf("sT", sizeof(float2) * slot * nw);
         // Potentials in chunks of kPotChunk slices: the first on the context stream, the rest on a
         // side stream, so that they are computed while the slice passes of earlier slices run (the
         // passes are latency bound and leave issue slots free); the row pass of the first slice of
         // each chunk waits for that chunk's event.  With per-launch profiling on, all run in order.
-        PotChunks pc = launch_potential_chunks(c, pot_args(p, s, A, g, sV, slot, 0, g.S_cap, 0), nw, g.S_cap);
+        PotChunks pc = launch_potential_chunks(c, with_transmission(pot_args(p, s, A, g, nullptr, slot, 0, g.S_cap, 0),
+                                                                    sT, s),
+                                               nw, g.S_cap);
         std::vector<WaveInfo> wv(nw);
         for (int i = 0; i < nw; i++) {
             wv[i].px = p.iw_x;
@@ -781,7 +794,8 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * nw);
         CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nw, cudaMemcpyHostToDevice, st));
         float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * nw);
-        PassArgs pa = pass_args(s, psi, dwv, sV, slot, cond);
+        PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
+        pa.tt = sT;
         if (iw == MS_IW_CONVERGENT) {
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_PROBE_INV, pa, nw, p.nx, st);
@@ -1050,13 +1064,13 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
         SpecGroup g = build_specimen(c, p, A, std::vector<int>{conf}, s.ph);
         const int S = g.ns[0];
         const double cc10 = gate_coef(-kPi * (p.cond_lens.c10 + g.z_init[0]) * s.ph.lambda);
-        float* sV;
+        float2* sT;
         int64_t slot = (int64_t)S * N;
         if (!plain) {
-            sV = (float*)c->buf("sV", sizeof(float) * slot);
-            run_potential(c, pot_args(p, s, A, g, sV, slot, 0, S, 0), 1, st);
+            sT = (float2*)c->buf("sT", sizeof(float2) * slot);
+            run_potential(c, with_transmission(pot_args(p, s, A, g, nullptr, slot, 0, S, 0), sT, s), 1, st);
         } else {
-            sV = (float*)c->buf("sV1", sizeof(float) * N);
+            sT = (float2*)c->buf("sT1", sizeof(float2) * N);
         }
         // every scan position of this configuration, uploaded once (run_STEM_tile_simu's tile loop,
         // scan_simulator.cuh:57-104, without a host round trip per batch)
@@ -1073,7 +1087,8 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
         WaveInfo* dwv_all = (WaveInfo*)c->buf("waves_all", sizeof(WaveInfo) * npos);
         CK(cudaMemcpyAsync(dwv_all, wv.data(), sizeof(WaveInfo) * npos, cudaMemcpyHostToDevice, st));
         if (!tuned) {
-            PassArgs base = pass_args(s, nullptr, nullptr, sV, slot, cond);
+            PassArgs base = pass_args(s, nullptr, nullptr, nullptr, slot, cond);
+            base.tt = sT;
             B = autotune_batch(c, p, s, base, wv[0], S, npos, cap);
             tuned = true;
         }
@@ -1084,7 +1099,8 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
         for (int start = 0; start < npos; start += B) {
             const int nb = std::min(B, npos - start);
             CK(cudaMemcpyAsync(dwv, dwv_all + start, sizeof(WaveInfo) * nb, cudaMemcpyDeviceToDevice, st));
-            PassArgs pa = pass_args(s, psi, dwv, sV, plain ? 0 : slot, cond);
+            PassArgs pa = pass_args(s, psi, dwv, nullptr, plain ? 0 : slot, cond);
+            pa.tt = sT;
             if (!plain) {
                 auto body = [&] {
                     PassArgs q = pa;
@@ -1112,7 +1128,7 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
             run_col(c, p.ny, COL_PROBE_INV, pa, nb, p.nx, st);
             for (int sl = 0; sl < S; sl++) {
                 pa.slice = sl;
-                run_potential(c, pot_args(p, s, A, g, sV, 0, sl, 1, sl), 1, st);
+                run_potential(c, with_transmission(pot_args(p, s, A, g, nullptr, 0, sl, 1, sl), sT, s), 1, st);
                 pa.sV_slice_base = sl;
                 pa.tw = s.tw_x;
                 run_row(c, p.nx, ROW_INV_T_FWD, pa, nb, p.ny, st);
@@ -1180,8 +1196,8 @@ void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* 
         SpecGroup g = build_specimen(c, p, A, std::vector<int>{conf}, s.ph);
         const int S = g.ns[0];
         const int64_t slot = (int64_t)S * N;
-        float* sV = (float*)c->buf("sV", sizeof(float) * slot);
-        run_potential(c, pot_args(p, s, A, g, sV, slot, 0, S, 0), 1, st);
+        float2* sT = (float2*)c->buf("sT", sizeof(float2) * slot);
+        run_potential(c, with_transmission(pot_args(p, s, A, g, nullptr, slot, 0, S, 0), sT, s), 1, st);
         WaveInfo wv;
         wv.px = p.iw_x;
         wv.py = p.iw_y;
@@ -1194,7 +1210,8 @@ void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* 
         CK(cudaMemcpyAsync(dwv, &wv, sizeof(WaveInfo), cudaMemcpyHostToDevice, st));
         float2* psi = (float2*)c->buf("psi", sizeof(float2) * N);
         float2* aux = (float2*)c->buf("aux", sizeof(float2) * N);
-        PassArgs pa = pass_args(s, psi, dwv, sV, slot, cond);
+        PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
+        pa.tt = sT;
         pa.aux = aux;
         pa.filt_g2in = g2in;
         pa.filt_g2out = g2out;
@@ -1591,6 +1608,20 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
         size_t budget = free_budget(), used = 0;
         int r1 = r0;
         while (r1 < n && (r1 == r0 || used + need[r1] <= budget)) used += need[r1++];
+        // one arena, cached in the context like every other buffer, holds the round's per-instance
+        // potential stores, propagator tables and patterns (bump allocation, 256-byte aligned);
+        // an instance whose store outgrows its estimate gets a buffer of its own
+        unsigned char* arena = (unsigned char*)c->buf("many_arena", used);
+        size_t arena_off = 0;
+        auto take = [&](const std::string& name, size_t bytes) -> void* {
+            bytes = (bytes + 255) / 256 * 256;
+            if (arena_off + bytes <= used) {
+                void* p = arena + arena_off;
+                arena_off += bytes;
+                return p;
+            }
+            return c->buf(name, bytes);
+        };
         // ---- phase 1 (context stream): specimens, potentials, propagators
         for (int i = r0; i < r1; i++) {
             const ms_params& p = ps[i];
@@ -1619,12 +1650,12 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             SpecGroup g = build_specimen(c, p, A, cs.confs, ph);
             I.nconf = g.nconf;
             const int64_t slot = (int64_t)g.S_cap * N;
-            I.sV = (float*)c->buf("many_sV_" + std::to_string(i), sizeof(float) * slot * g.nconf);
+            I.sV = (float*)take("many_sV_" + std::to_string(i), sizeof(float) * slot * g.nconf);
             run_potential(c, pot_args(p, s0, A, g, I.sV, slot, 0, g.S_cap, 0), g.nconf, st);
-            I.prop = (float2*)c->buf("many_prop_" + std::to_string(i), sizeof(float2) * N);
+            I.prop = (float2*)take("many_prop_" + std::to_string(i), sizeof(float2) * N);
             launch_prop_table(p.nx, p.ny, gc.dgx, gc.dgy, gc.g0x, gc.g0y, gc.prop_w, gc.alpha, gc.gl2, p.bwl ? 1 : 0,
                               I.prop, st);
-            I.out = (float*)c->buf("many_out_" + std::to_string(i), sizeof(float) * N);
+            I.out = (float*)take("many_out_" + std::to_string(i), sizeof(float) * N);
             I.waves.assign((size_t)g.nconf, WaveInfo());
             I.S_max = 0;
             for (int k = 0; k < g.nconf; k++) {
@@ -1671,7 +1702,7 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             twiddles(c, G.nx);
             twiddles(c, G.ny);
         }
-        cudaEvent_t fork = c->prof_event();
+        cudaEvent_t fork = chunk_event(c, 0);
         CK(cudaEventRecord(fork, st));
         for (size_t gi = 0; gi < groups.size(); gi++) {
             Group& G = groups[gi];
@@ -1738,20 +1769,19 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
                 }
             }
         }
-        for (Group& G : groups) {
-            cudaEvent_t j = c->prof_event();
-            CK(cudaEventRecord(j, G.s));
+        for (size_t gi = 0; gi < groups.size(); gi++) {
+            cudaEvent_t j = chunk_event(c, 1 + gi);
+            CK(cudaEventRecord(j, groups[gi].s));
             CK(cudaStreamWaitEvent(st, j, 0));
         }
         for (int i = r0; i < r1; i++) copy_out(c, outs[i].image_intensity, in[i].out, (int64_t)ps[i].nx * ps[i].ny,
                                                outs[i].on_device);
         CK(cudaStreamSynchronize(st));
-        c->ev_used = 0;
-        // a later round reuses buffer names; drop this round's stores
+        // buffers of instances that outgrew the arena are this call's alone
         for (int i = r0; i < r1; i++) {
             for (const char* nm : {"many_sV_", "many_prop_", "many_out_"}) {
                 auto it = c->bufs.find(nm + std::to_string(i));
-                if (it != c->bufs.end() && r1 < n) {
+                if (it != c->bufs.end()) {
                     cudaFree(it->second.p);
                     c->bufs.erase(it);
                 }

@@ -41,6 +41,7 @@ struct FftLayout {
     static constexpr int ROW_THREADS = ROWS * G;
     static constexpr int COL_THREADS = TC * G;
     static constexpr int COL_MINB = (N == 2048) ? 1 : 2;   // resident column blocks per SM (register cap)
+    static constexpr bool COL_TW_GLOBAL = false;            // twiddles staged in shared memory
     static constexpr int ROW_MINB = (N == 2048) ? 1 : 2;   // resident row blocks per SM (register cap)
     // transpose scratch of one transform: E rows of G+1 slots, plus padding so that
     // consecutive transforms start on banks that keep a half-warp conflict-free
@@ -50,7 +51,7 @@ struct FftLayout {
         (TC == 16) ? (SCR_BASE + ((1 - SCR_BASE % 16) + 16) % 16) : (SCR_BASE + ((2 - SCR_BASE % 16) + 16) % 16);
     // transpose scratch, twiddles (high and low parts), and the 1024-entry exp(i phi) table
     static constexpr size_t ROW_SMEM = sizeof(float2) * ((size_t)ROWS * SCR_STRIDE_ROW + 2 * N + 1024);
-    static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + 2 * N);
+    static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + (COL_TW_GLOBAL ? 0 : 2 * N));
 };
 
 }  // namespace msb

@@ -12,9 +12,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
 #include <mutex>
-#include <set>
-#include <tuple>
+#include <utility>
 #include <cfloat>
 
 #include "detmath.cuh"
@@ -30,25 +30,24 @@ void reset_kernel_launches() { g_launches.store(0); }
 void add_kernel_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 static inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-// Raises a kernel's dynamic shared-memory limit once per device and size (the attribute stays
-// set for the process) instead of before every launch: the slice loop launches thousands of
-// kernels per call and the host must keep ahead of them.
+// Raises a kernel's dynamic shared-memory limit only when a launch needs more than the limit
+// already set on this device (the attribute stays set for the process), instead of before every
+// launch: the slice loop launches thousands of kernels per call and the host must keep ahead of
+// them.  The limit is only ever raised: setting it lowers it too, below sizes launched before.
 static std::mutex g_attr_mtx;
-static std::set<std::tuple<int, const void*, size_t>> g_attr_done;
+static std::map<std::pair<int, const void*>, size_t> g_attr_max;
 
 template <class F>
 static void smem_attr(F* kernel, size_t bytes)
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const auto key = std::make_tuple(dev, (const void*)kernel, bytes);
-    {
-        std::lock_guard<std::mutex> lk(g_attr_mtx);
-        if (g_attr_done.count(key)) return;
-    }
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    const auto key = std::make_pair(dev, (const void*)kernel);
     std::lock_guard<std::mutex> lk(g_attr_mtx);
-    g_attr_done.insert(key);
+    auto it = g_attr_max.find(key);
+    if (it != g_attr_max.end() && it->second >= bytes) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    g_attr_max[key] = bytes;
 }
 
 static void check_launch(const char* what)
@@ -151,30 +150,33 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
     const int r = (blockIdx.x % blocks_per_wave) * L::ROWS + team;
     const WaveInfo wi = a.waves[b];
     const bool beyond = a.slice >= wi.n_slices;
-    if ((OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X) && beyond && !(a.flags & PF_VACUUM_BEYOND))
-        return;
+    constexpr bool kT = OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_INV_TT_FWD ||
+                        OP == ROW_TT_FWD;
+    constexpr bool kTT = OP == ROW_INV_TT_FWD || OP == ROW_TT_FWD;
+    if (kT && beyond && !(a.flags & PF_VACUUM_BEYOND)) return;
 
     const size_t row_off = ((size_t)b * ny + r) * N;
     float2 v[E];
     // the wave's loads go out first, so their latency overlaps the table staging below
-    if (OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_ADJ) {
+    if (OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_INV_TT_FWD || OP == ROW_ADJ) {
 #pragma unroll
         for (int j = 0; j < E; j++) v[j] = a.psi[row_off + g + G * j];
     }
     float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
     float2* etab = tw + 2 * N;
     for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_ADJ)
+    if ((kT && !kTT) || OP == ROW_ADJ)
         for (int i = threadIdx.x; i < kExpTab; i += blockDim.x) etab[i] = a.exptab[i];
     __syncthreads();
     float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
     auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
     auto sync = []() { __syncwarp(); };
 
-    if (OP == ROW_T_FWD || OP == ROW_INV_T_FWD || OP == ROW_INV_T_FWD_X || OP == ROW_ADJ) {
-        const float* vr = (wi.sV ? wi.sV : a.sV + (size_t)wi.conf_slot * a.sV_slot_stride) +
-                          ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
-        if (OP == ROW_T_FWD) {
+    if (kT || OP == ROW_ADJ) {
+        const size_t voff = ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N;
+        const float* vr = kTT ? nullptr : (wi.sV ? wi.sV : a.sV + (size_t)wi.conf_slot * a.sV_slot_stride) + voff;
+        const float2* tr = kTT ? a.tt + (size_t)wi.conf_slot * a.sV_slot_stride + voff : nullptr;
+        if (OP == ROW_T_FWD || OP == ROW_TT_FWD) {
 #pragma unroll
             for (int j = 0; j < E; j++) v[j] = make_float2(1.0f, 0.0f);
         }
@@ -184,7 +186,7 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
         // adjoint wave and x = t psi the stored forward wave, dL/dV += Re(i x conj(xbar)) and the
         // adjoint continues as conj(t) xbar (or_stem_backward's chain, restated per row).
 #pragma unroll 1
-        for (int pass = (OP == ROW_T_FWD) ? 1 : 0; pass < 2; pass++) {
+        for (int pass = (OP == ROW_T_FWD || OP == ROW_TT_FWD) ? 1 : 0; pass < 2; pass++) {
             if (pass == 0) conj_all(v);
             else if (OP == ROW_ADJ) {
                 const float2* xr = a.xs + row_off;
@@ -196,8 +198,13 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
                     v[j] = cmulc(v[j], expi_tab(__ldg(vr + g + G * j), etab));
                 }
             } else if (!beyond) {
+                if constexpr (kTT) {
 #pragma unroll
-                for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + g + G * j), etab));
+                    for (int j = 0; j < E; j++) v[j] = cmul(v[j], __ldg(tr + g + G * j));
+                } else {
+#pragma unroll
+                    for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + g + G * j), etab));
+                }
                 if constexpr (OP == ROW_INV_T_FWD_X) {
 #pragma unroll
                     for (int j = 0; j < E; j++) a.xs[row_off + g + G * j] = v[j];
@@ -264,9 +271,15 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
 #pragma unroll
         for (int j = 0; j < E; j++) v[j] = cp[j * cs];
     }
-    float2* tw = smem + TC * L::SCR_STRIDE_COL;
-    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
-    __syncthreads();
+    const float2* tw;
+    if constexpr (L::COL_TW_GLOBAL) {
+        tw = a.tw;   // read through L1: shared memory is kept for the transposes of three blocks per SM
+    } else {
+        float2* tws = smem + TC * L::SCR_STRIDE_COL;
+        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tws[i] = a.tw[i];
+        __syncthreads();
+        tw = tws;
+    }
     float2* scr_base = smem + c * L::SCR_STRIDE_COL;
     auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
     auto sync = []() { __syncthreads(); };
@@ -707,12 +720,14 @@ static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStre
 {
     using L = FftLayout<N>;
     // the pipelined form copies potential rows with 16-byte cp.async: it needs an aligned store
-    if (op == ROW_INV_T_FWD && a.variant == PASS_PIPELINED && !(a.flags & PF_STORE_X) &&
+    if (op == ROW_INV_T_FWD && a.variant == PASS_PIPELINED && !(a.flags & PF_STORE_X) && !a.tt && a.sV &&
         ((uintptr_t)a.sV & 15) == 0 && row_pipe<N>(a, nwaves, ny, st))
         return;
     dim3 grid((unsigned)(nwaves * (ny / L::ROWS))), block(L::ROW_THREADS);
     size_t sm = L::ROW_SMEM;
     if (op == ROW_INV_T_FWD && (a.flags & PF_STORE_X)) op = ROW_INV_T_FWD_X;
+    else if (a.tt && op == ROW_INV_T_FWD) op = ROW_INV_TT_FWD;
+    else if (a.tt && op == ROW_T_FWD) op = ROW_TT_FWD;
     switch (op) {
     case ROW_T_FWD:
         smem_attr(k_row<N, ROW_T_FWD>, sm);
@@ -737,6 +752,14 @@ static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStre
     case ROW_INV_T_FWD_X:
         smem_attr(k_row<N, ROW_INV_T_FWD_X>, sm);
         k_row<N, ROW_INV_T_FWD_X><<<grid, block, sm, st>>>(a);
+        break;
+    case ROW_INV_TT_FWD:
+        smem_attr(k_row<N, ROW_INV_TT_FWD>, sm);
+        k_row<N, ROW_INV_TT_FWD><<<grid, block, sm, st>>>(a);
+        break;
+    case ROW_TT_FWD:
+        smem_attr(k_row<N, ROW_TT_FWD>, sm);
+        k_row<N, ROW_TT_FWD><<<grid, block, sm, st>>>(a);
         break;
     default: throw MsError(MS_ERR_INTERNAL, "unknown row pass");
     }
@@ -1140,9 +1163,20 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
     }
 #pragma unroll
     for (int r = 0; r < RY; r++) {
-        float* out = a.V + (int64_t)conf * a.V_conf_stride + (int64_t)(sl - a.V_slice_base) * a.nx * a.ny +
-                     (int64_t)(ty0 + py + r * ROW_STEP) * a.nx + tx0 + 4 * px;
-        *reinterpret_cast<float4*>(out) = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+        const int64_t o = (int64_t)conf * a.V_conf_stride + (int64_t)(sl - a.V_slice_base) * a.nx * a.ny +
+                          (int64_t)(ty0 + py + r * ROW_STEP) * a.nx + tx0 + 4 * px;
+        if (a.T) {
+            // the transmission function t = exp(i V) of the four pixels, as the row pass would form it
+            // (transmission_function.cuh:107-119), so the slice passes read t instead of V
+            float2 t[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) t[k] = expi_tab(acc[r][k], a.exptab);
+            float4* out = reinterpret_cast<float4*>(a.T + o);
+            out[0] = make_float4(t[0].x, t[0].y, t[1].x, t[1].y);
+            out[1] = make_float4(t[2].x, t[2].y, t[3].x, t[3].y);
+        } else {
+            *reinterpret_cast<float4*>(a.V + o) = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+        }
     }
 }
 

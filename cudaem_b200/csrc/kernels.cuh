@@ -47,7 +47,9 @@ enum RowOp {
     ROW_INV_ABS2 = 2,
     ROW_INV_STORE = 3,
     ROW_ADJ = 4,
-    ROW_INV_T_FWD_X = 5   // ROW_INV_T_FWD that also keeps t psi in xs (selected by PF_STORE_X)
+    ROW_INV_T_FWD_X = 5,  // ROW_INV_T_FWD that also keeps t psi in xs (selected by PF_STORE_X)
+    ROW_INV_TT_FWD = 6,   // ROW_INV_T_FWD with t = exp(i V) read from a transmission store (selected by tt)
+    ROW_TT_FWD = 7        // ROW_T_FWD likewise
 };
 enum ColOp {
     COL_PROBE_INV = 0,
@@ -76,7 +78,8 @@ struct PassArgs {
     int slice;
     int flags;
     const float* sV;          // potential store, [slot][slice][ny][nx], rad
-    int64_t sV_slot_stride;   // floats per slot
+    const float2* tt;         // or, if set, the transmission store exp(i sV) with the same layout
+    int64_t sV_slot_stride;   // elements per slot
     int sV_slice_base;        // slice index held at the store's slice 0
     const float2* tw;         // inter-level twiddles for this pass's length
     const float2* prop_x;     // [nx] exp(i w (gx - g0x)^2)
@@ -132,6 +135,8 @@ struct PotArgs {
     const ElemTable* elems;
     int n_elem;
     const float4* pair_coef;    // fine slicing: spline coefficients of every sorted (atom, slice) pair
+    float2* T;                  // if set: write the transmission exp(i V) here instead of V
+    const float2* exptab;       // [1024] exp(2 pi i k / 1024) for the transmission
 };
 
 struct ElemCoefDev;

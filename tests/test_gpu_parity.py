@@ -152,3 +152,14 @@ def test_thickness_convergent_phonons(ctx):
     out = cb.ThicknessSimulator(ctx=ctx).run(p, at)
     ref = orc.simulate_thickness(p, at)
     assert rel_l2(out.thickness_frames, ref) < TOL
+
+
+def test_kernel_limits_survive_switching_specimens(ctx):
+    """Launch-size bookkeeping across calls: three-element, one-element, then three-element
+    specimens again in one context (the potential kernel's shared memory grows with the number
+    of elements) all run and match the oracle."""
+    for maker in (cases.hrtem_small, cases.cbed_small, cases.hrtem_small):
+        p, at = maker()
+        V = ctx.projected_potential(p, at, conf=0)
+        Vo, _ = orc.potential(p, at, 0)
+        assert rel_l2(V, Vo) < TOL_POT
