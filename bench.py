@@ -350,6 +350,10 @@ def run_ours(args):
     launches = 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
+        # one more untimed step while the clock sampler starts (its start-up competes for the
+        # host cores that issue the launches)
+        step(co)
+        torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()

@@ -1023,10 +1023,13 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
         // margin of one pixel for the float rounding of the block corners
         const float WX0 = (float)(tx0 + (wblk % 4) * 16 - 1) * a.dx, WX1 = (float)(tx0 + (wblk % 4) * 16 + 16) * a.dx;
         const float WY0 = (float)(ty0 + (wblk / 4) * 16 - 1) * a.dy, WY1 = (float)(ty0 + (wblk / 4) * 16 + 16) * a.dy;
-        if (t == 0) {
+        if (t < 32) {
             // Atoms are sorted by (configuration, slice, cell) with cells of a.cell A in a
             // ncx x ncy grid over the box.  The tile needs the cells its rectangle, grown by the
             // largest cut-off, touches: one contiguous key range per cell row and periodic image.
+            // Warp 0 looks the ranges up in parallel (one (row, image) item per lane) and keeps the
+            // non-empty ones in item order, with their running atom counts.
+            const int lane = t;
             const float R = a.rmax_all * 1.0001f + 1e-4f;
             int cx0 = (int)floorf((X0 - R) * a.inv_cell), cx1 = (int)floorf((X1 + R) * a.inv_cell);
             int cy0 = (int)floorf((Y0 - R) * a.inv_cell), cy1 = (int)floorf((Y1 + R) * a.inv_cell);
@@ -1037,27 +1040,54 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
                 cy1 = min(cy1, a.ncy - 1);
             }
             const int64_t key_base = ((int64_t)conf * (a.S_cap + 1) + sl) * a.ncx * a.ncy;
+            // the column range split at the box's periodic boundaries (at most three pieces)
+            int xs_b[3], xs_e[3], xs_o[3], nxs = 0;
+            for (int cx = cx0; cx <= cx1 && nxs < 3;) {
+                const int ox = a.wrap ? floordiv_i(cx, a.ncx) : 0;
+                const int end = min(cx1, (ox + 1) * a.ncx - 1);
+                xs_b[nxs] = cx;
+                xs_e[nxs] = end;
+                xs_o[nxs] = ox;
+                nxs++;
+                cx = end + 1;
+            }
+            const int n_items = (cy1 >= cy0) ? (cy1 - cy0 + 1) * nxs : 0;
             int nr = 0;
             unsigned run = 0;
-            r_pre[0] = 0;
-            for (int cy = cy0; cy <= cy1 && nr < kPotMaxRanges; cy++) {
-                const int oy = a.wrap ? floordiv_i(cy, a.ncy) : 0, cyw = cy - oy * a.ncy;
-                int cx = cx0;
-                while (cx <= cx1 && nr < kPotMaxRanges) {
-                    const int ox = a.wrap ? floordiv_i(cx, a.ncx) : 0, cxw = cx - ox * a.ncx;
-                    const int end = min(cx1, (ox + 1) * a.ncx - 1);
+            for (int base = 0; base < n_items && nr < kPotMaxRanges; base += 32) {
+                const int it = base + lane;
+                unsigned b0 = 0, b1 = 0;
+                int img = 0;
+                if (it < n_items) {
+                    const int cy = cy0 + it / nxs, xi = it % nxs;
+                    const int oy = a.wrap ? floordiv_i(cy, a.ncy) : 0, cyw = cy - oy * a.ncy;
+                    const int cxw = xs_b[xi] - xs_o[xi] * a.ncx;
                     const int64_t k0 = key_base + (int64_t)cyw * a.ncx + cxw;
-                    const unsigned b0 = a.seg[k0], b1 = a.seg[k0 + (end - cx) + 1];
-                    if (b1 > b0) {
-                        r_beg[nr] = b0;
-                        r_img[nr] = (ox + 8) | ((oy + 8) << 8);
-                        run += b1 - b0;
-                        r_pre[++nr] = run;
-                    }
-                    cx = end + 1;
+                    b0 = a.seg[k0];
+                    b1 = a.seg[k0 + (xs_e[xi] - xs_b[xi]) + 1];
+                    img = (xs_o[xi] + 8) | ((oy + 8) << 8);
                 }
+                const bool ok = b1 > b0;
+                const unsigned mask = __ballot_sync(0xffffffffu, ok);
+                const int pos = nr + __popc(mask & ((1u << lane) - 1u));
+                unsigned incl = ok ? b1 - b0 : 0u;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                if (ok && pos < kPotMaxRanges) {
+                    r_beg[pos] = b0;
+                    r_img[pos] = img;
+                    r_pre[pos + 1] = run + incl;
+                }
+                nr = min(nr + __popc(mask), kPotMaxRanges);
+                run += __shfl_sync(0xffffffffu, incl, 31);
             }
-            n_ranges = nr;
+            if (lane == 0) {
+                r_pre[0] = 0;
+                n_ranges = nr;
+            }
         }
         __syncthreads();
         const int nr = n_ranges;
