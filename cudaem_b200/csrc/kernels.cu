@@ -562,6 +562,111 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_row_p(PassArgs a, int nwave
     cp_async_wait_all();
 }
 
+// Row pass on a transmission store (ROW_INV_TT_FWD), 12 warps per SM.  One persistent block of
+// 384 threads per SM; each warp walks its rows with a grid stride and double-buffers them in
+// shared memory: while a row is transformed, the next one arrives by cp.async (no registers, no
+// wait until it is needed), and the buffer a row arrived in serves as its transposition scratch
+// (XOR-swizzled so that the N points fill exactly N slots without bank conflicts).  The row's
+// transmission values are loaded into registers before the inverse transform and consumed after
+// it.  The arithmetic is the classic kernel's.
+constexpr int kQWarps = 12;
+int num_sms();
+
+template <int N>
+__global__ void __launch_bounds__(kQWarps * 32, 1) k_row_q(PassArgs a, int nwaves)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E;
+    constexpr int R = 32 / G;        // rows per warp item (one per team)
+    constexpr int ITEM = R * N;      // float2 of one item
+    extern __shared__ float2 smem[];
+    float2* tw = smem;
+    for (int i = threadIdx.x; i < 2 * N; i += kQWarps * 32) tw[i] = a.tw[i];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tm = lane / G, g = lane % G;
+    float2* wbuf = smem + 2 * N + (size_t)warp * 2 * ITEM;
+    __syncthreads();
+    const int ny = a.grid.ny;
+    const int64_t n_items = (int64_t)nwaves * ny / R;
+    const int64_t stride = (int64_t)gridDim.x * kQWarps;
+    const bool vac = (a.flags & PF_VACUUM_BEYOND) != 0;
+    auto next_live = [&](int64_t it) {
+        while (it < n_items && !vac && a.slice >= a.waves[(int)((it * R) / ny)].n_slices) it += stride;
+        return it;
+    };
+    auto t_item = [&](int64_t it) -> const float2* {
+        const int64_t row0 = it * R;
+        const WaveInfo& wi = a.waves[(int)(row0 / ny)];
+        if (a.slice >= wi.n_slices) return nullptr;
+        return a.tt + (size_t)wi.conf_slot * a.sV_slot_stride +
+               ((size_t)(a.slice - a.sV_slice_base) * ny + (int)(row0 % ny)) * N;
+    };
+    // the item's wave rows into dst by cp.async; its transmission rows towards L2 (they are read
+    // after the first transform, so a register copy would only raise the register count)
+    auto fetch = [&](int64_t it, float2* dst) {
+        const float2* src = a.psi + it * ITEM;
+        for (int q = lane; q < ITEM / 2; q += 32) cp_async16(dst + 2 * q, src + 2 * q);
+        cp_async_commit();
+        if (const float2* tr = t_item(it))
+            for (int q = lane; q < ITEM / 16; q += 32)
+                asm volatile("prefetch.global.L2 [%0];\n" ::"l"(tr + 16 * q));
+    };
+    int64_t it = next_live((int64_t)blockIdx.x * kQWarps + warp);
+    int cur = 0;
+    if (it < n_items) fetch(it, wbuf);
+    while (it < n_items) {
+        cp_async_wait_all();
+        __syncwarp();
+        float2* B = wbuf + cur * ITEM;
+        float2 v[E];
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = B[tm * N + g + G * j];
+        const int64_t nxt = next_live(it + stride);
+        // the other buffer was the previous item's scratch; every lane is past its last use
+        if (nxt < n_items) fetch(nxt, wbuf + (cur ^ 1) * ITEM);
+        const int64_t row = it * R + tm;
+        const float2* tr = t_item(it);
+        if (tr) tr += (size_t)tm * N;
+        float2* scr_base = B + tm * N;
+        auto scr = [scr_base](int k1, int q) { return scr_base + k1 * G + (q ^ (k1 & (G - 1))); };
+        auto sync = []() { __syncwarp(); };
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {
+            if (pass == 0) conj_all(v);
+            else if (tr) {
+#pragma unroll
+                for (int j = 0; j < E; j++) v[j] = cmul(v[j], __ldg(tr + g + G * j));
+            }
+            team_fft<N, G, -1>(v, g, tw, scr, sync);
+            if (pass == 0) conj_all(v);
+        }
+        float2* dst = a.psi + row * N;
+#pragma unroll
+        for (int j = 0; j < E; j++) dst[g + G * j] = v[j];
+        __syncwarp();
+        cur ^= 1;
+        it = nxt;
+    }
+    cp_async_wait_all();
+}
+
+template <int N>
+static bool row_q(const PassArgs& a, int nwaves, int ny, cudaStream_t st)
+{
+    if constexpr (N != 512 && N != 1024) {
+        return false;
+    } else {
+        using L = FftLayout<N>;
+        constexpr int R = 32 / L::G;
+        const int64_t items = (int64_t)nwaves * ny / R;
+        const int64_t blocks = std::min<int64_t>((items + kQWarps - 1) / kQWarps, num_sms());
+        const size_t sm = sizeof(float2) * (2 * (size_t)N + (size_t)kQWarps * 2 * R * N);
+        smem_attr(k_row_q<N>, sm);
+        k_row_q<N><<<(unsigned)blocks, kQWarps * 32, sm, st>>>(a, nwaves);
+        return true;
+    }
+}
+
 template <int N>
 __global__ void __launch_bounds__(kPipeThreads, 1) k_col_p(PassArgs a, int nwaves)
 {
@@ -728,6 +833,10 @@ static void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStre
     if (op == ROW_INV_T_FWD && (a.flags & PF_STORE_X)) op = ROW_INV_T_FWD_X;
     else if (a.tt && op == ROW_INV_T_FWD) op = ROW_INV_TT_FWD;
     else if (a.tt && op == ROW_T_FWD) op = ROW_TT_FWD;
+    // the 12-warp form copies wave rows with 16-byte cp.async: it needs an aligned wave
+    if (op == ROW_INV_TT_FWD && a.variant == PASS_PIPELINED && ((uintptr_t)a.psi & 15) == 0 &&
+        row_q<N>(a, nwaves, ny, st))
+        return;
     switch (op) {
     case ROW_T_FWD:
         smem_attr(k_row<N, ROW_T_FWD>, sm);

@@ -4,9 +4,11 @@ Both kernel forms run the same transform code on the same data; only the schedul
 (persistent blocks, prefetching) and the compiler's contraction of a few products differ,
 so every output agrees to float rounding (relative L2 <= 1e-6; the adjoint's loss and
 gradients, which carry residuals 30x smaller than the intensities, to 1e-4).  Covered:
-square grids 128..2048 (2048 falls back to the classic form), a rectangular grid, more waves than resident blocks, phonon configurations with different
-slice counts (items skipped mid-pass), the adjoint's conjugate propagator step, and the
-uneven batch's per-wave potential and propagator tables.
+square grids 128..2048 (2048 falls back to the classic form), a rectangular grid, more waves than
+resident blocks, phonon configurations with different slice counts (items skipped mid-pass), the
+row pass on a transmission store at 512 and 1024 points (CBED, thickness series, uneven batch),
+the adjoint's conjugate propagator step, and the uneven batch's per-wave potential and
+propagator tables.
 """
 import os
 import sys
@@ -55,10 +57,20 @@ def test_slice_loop_agree(ctx, nx, ny, n_probe):
     assert _close(a, b)
 
 
-def test_cbed_phonons_agree(ctx):
-    p, at = cases.cbed_small(n=256, cells=(3, 3, 5), nconf=5)
+@pytest.mark.parametrize("n,nconf", [(256, 5), (512, 3), (1024, 2)])
+def test_cbed_phonons_agree(ctx, n, nconf):
+    # 512 and 1024 run the row pass on the transmission store in the 12-warp double-buffered form
+    p, at = cases.cbed_small(n=n, cells=(3, 3, 5), nconf=nconf)
     sim = cb.MulSimulator(ctx=ctx)
     a, b = _both(ctx, lambda: sim.executionCBED(p, at).image_intensity)
+    assert _close(a, b)
+
+
+@pytest.mark.parametrize("n", [512, 1024])
+def test_thickness_agree(ctx, n):
+    p, at = cases.thickness_small(n=n)
+    sim = cb.ThicknessSimulator(ctx=ctx)
+    a, b = _both(ctx, lambda: sim.run(p, at).thickness_frames)
     assert _close(a, b)
 
 
@@ -78,6 +90,8 @@ def test_adjoint_agree(ctx):
 def test_uneven_batch_agree(ctx):
     jobs = [wl.cbed_si(cells=(2, 2, 3), n=256, nconf=2, seed=s) for s in (1, 2)]
     jobs.append(wl.cbed_si(cells=(2, 2, 5), n=128, nconf=1, seed=3))
+    jobs.append(wl.cbed_si(cells=(2, 2, 4), n=512, nconf=2, seed=4))
+    jobs.append(wl.cbed_si(cells=(2, 2, 2), n=1024, nconf=1, seed=5))
     sim = cb.MulSimulator(ctx=ctx)
     a, b = _both(ctx, lambda: [o.image_intensity for o in sim.executionMany(jobs)[0]])
     for x, y in zip(a, b):
