@@ -52,6 +52,8 @@ def parse():
                     help="skip the batched-vs-plain, adjoint and uneven-batch measurements")
     ap.add_argument("--pass-kernels", type=int, default=0, choices=[0, 1],
                     help="slice-pass kernel form: 0 classic (default), 1 persistent pipelined")
+    ap.add_argument("--potential-overlap", type=int, default=0, choices=[0, 1],
+                    help="potentials: 0 all before the slice loop (default), 1 in chunks beside the slice passes")
     ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
     ap.add_argument("--nconf", type=int, default=0, help="phonon configurations (0: the workload's)")
     return ap.parse_args()
@@ -320,6 +322,7 @@ def run_ours(args):
         desc = dict(desc, workload=desc["workload"] + f" [reduced: cells_z={args.cells_z}, nconf={args.nconf}]")
     ctx = cb.Context(local)
     ctx.set_pass_kernels(args.pass_kernels)
+    ctx.set_potential_overlap(bool(args.potential_overlap))
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     L = cb.lib()

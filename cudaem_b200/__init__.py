@@ -266,6 +266,11 @@ class Context:
         """0: classic one-block-per-tile slice passes (default); 1: persistent pipelined passes."""
         self.check(lib().ms_set_pass_kernels(self.handle, variant))
 
+    def set_potential_overlap(self, enable: bool) -> None:
+        """False: all potentials before the slice loop (default); True: 16-slice chunks on a side
+        stream beside the slice passes.  Identical results."""
+        self.check(lib().ms_set_potential_overlap(self.handle, 1 if enable else 0))
+
     def set_profiling(self, enable: bool) -> None:
         self.check(lib().ms_set_profiling(self.handle, 1 if enable else 0))
 

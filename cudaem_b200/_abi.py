@@ -150,6 +150,7 @@ PROTOTYPES = {
     "ms_last_probe_batch": (C.c_int, [C.c_void_p]),
     "ms_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_set_pass_kernels": (C.c_int, [C.c_void_p, C.c_int]),
+    "ms_set_potential_overlap": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_simulate_many": (C.c_int, [C.c_void_p, C.c_int, _P(ms_params), _P(ms_atoms), _P(ms_output),
                                    _P(C.c_double)]),
 }

@@ -177,6 +177,13 @@ ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
     return MS_OK;
 }
 
+ms_status ms_set_potential_overlap(ms_ctx* c, int enable)
+{
+    if (!c) return MS_ERR_INVALID_ARG;
+    c->pot_overlap = enable != 0;
+    return MS_OK;
+}
+
 ms_status ms_set_graphs(ms_ctx* c, int enable)
 {
     if (!c) return MS_ERR_INVALID_ARG;

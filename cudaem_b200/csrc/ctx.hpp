@@ -37,6 +37,7 @@ struct ms_ctx {
     std::map<std::string, Graph> graphs;         // keyed by the launch arguments they bake in
     bool use_graphs = true;
     int pass_variant = 0;                        // msb::PassVariant of the slice-pass kernels (0: classic)
+    bool pot_overlap = false;                    // potential chunks on a side stream beside the slice passes
     int last_batch = 0;                          // probe batch used by the last STEM call
     std::vector<cudaStream_t> side;              // streams of the grid groups of an uneven batch
     cudaStream_t pot_stream = nullptr;           // potential chunks computed beside the slice passes

@@ -618,7 +618,7 @@ PotChunks launch_potential_chunks(ms_ctx* c, PotArgs a, int n_conf, int S)
 {
     PotChunks pc;
     const int nchunk = (S + kPotChunk - 1) / kPotChunk;
-    if (c->profile || nchunk <= 1) {
+    if (c->profile || nchunk <= 1 || !c->pot_overlap) {
         run_potential(c, a, n_conf, c->stream);
         return pc;
     }
@@ -774,10 +774,10 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         const int nw = g.nconf;
         const int64_t slot = (int64_t)g.S_cap * N;
         float2* sT = (float2*)c->buf("sT", sizeof(float2) * slot * nw);
-        // Potentials in chunks of kPotChunk slices: the first on the context stream, the rest on a
-        // side stream, so that they are computed while the slice passes of earlier slices run (the
-        // passes are latency bound and leave issue slots free); the row pass of the first slice of
-        // each chunk waits for that chunk's event.  With per-launch profiling on, all run in order.
+        // Potentials of every slice before the loop (default), or, with the overlap switched on, in
+        // chunks of kPotChunk slices: the first on the context stream, the rest on a side stream while
+        // the slice passes of earlier slices run; the row pass of the first slice of each chunk then
+        // waits for that chunk's event.  With per-launch profiling on, all run in order.
         PotChunks pc = launch_potential_chunks(c, with_transmission(pot_args(p, s, A, g, nullptr, slot, 0, g.S_cap, 0),
                                                                     sT, s),
                                                nw, g.S_cap);

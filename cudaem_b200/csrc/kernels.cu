@@ -1088,10 +1088,43 @@ __device__ __forceinline__ float spline_eval_c(const ElemTable& T, const float4*
 
 constexpr int kPotMaxRanges = 64;
 
-__device__ __forceinline__ int floordiv_i(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+// Cells of one axis that hold the atoms of the interval [lo, hi]: with periodic wrapping, one piece
+// per periodic image k that the interval reaches (at most three: a tile spans at most half the box
+// and the cut-off stays below half the box), each the interval shifted by -k L,
+// clipped to the box and turned into a cell range; without wrapping, one piece of cells clamped to
+// the grid (atoms outside the box sit in the edge cells).  Atoms are binned by
+// floor((x - k L) / cell) on the wrapped coordinate, so a range taken per image is exact even when
+// L is not a multiple of the cell size.  Returns the number of pieces; b/e are the first and last
+// cell, o the image.  Unrolled with constant indices, so the pieces stay in registers.
+__device__ __forceinline__ int cell_pieces(float lo, float hi, float L, int nc, float inv_cell, bool wrap, int (&b)[3],
+                                           int (&e)[3], int (&o)[3])
+{
+    int n = 0;
+    if (!wrap) {
+        b[0] = max((int)floorf(lo * inv_cell), 0);
+        e[0] = min((int)floorf(hi * inv_cell), nc - 1);
+        o[0] = 0;
+        return b[0] <= e[0] ? 1 : 0;
+    }
+    const int k0 = (int)floorf(lo / L), k1 = (int)floorf(hi / L);
+#pragma unroll
+    for (int piece = 0; piece < 3; piece++) {
+        const int k = k0 + piece;
+        const int c0 = max((int)floorf(fmaxf(lo - (float)k * L, 0.f) * inv_cell), 0);
+        const int c1 = min((int)floorf(fminf(hi - (float)k * L, L) * inv_cell), nc - 1);
+        if (k <= k1 && c0 <= c1) {
+            // n only grows, so pieces land at their own index or below (constant indices after unrolling)
+            if (n == 0) { b[0] = c0; e[0] = c1; o[0] = k; }
+            else if (n == 1) { b[1] = c0; e[1] = c1; o[1] = k; }
+            else { b[2] = c0; e[2] = c1; o[2] = k; }
+            n++;
+        }
+    }
+    return n;
+}
 
 template <bool FINE>
-__global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
+__global__ void __launch_bounds__(kPotThreads, 6) k_potential(PotArgs a)
 {
     extern __shared__ __align__(16) unsigned char psm[];
     ElemTable* el = reinterpret_cast<ElemTable*>(psm);
@@ -1140,27 +1173,15 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
             // non-empty ones in item order, with their running atom counts.
             const int lane = t;
             const float R = a.rmax_all * 1.0001f + 1e-4f;
-            int cx0 = (int)floorf((X0 - R) * a.inv_cell), cx1 = (int)floorf((X1 + R) * a.inv_cell);
-            int cy0 = (int)floorf((Y0 - R) * a.inv_cell), cy1 = (int)floorf((Y1 + R) * a.inv_cell);
-            if (!a.wrap) {
-                cx0 = max(cx0, 0);
-                cy0 = max(cy0, 0);
-                cx1 = min(cx1, a.ncx - 1);
-                cy1 = min(cy1, a.ncy - 1);
-            }
             const int64_t key_base = ((int64_t)conf * (a.S_cap + 1) + sl) * a.ncx * a.ncy;
-            // the column range split at the box's periodic boundaries (at most three pieces)
-            int xs_b[3], xs_e[3], xs_o[3], nxs = 0;
-            for (int cx = cx0; cx <= cx1 && nxs < 3;) {
-                const int ox = a.wrap ? floordiv_i(cx, a.ncx) : 0;
-                const int end = min(cx1, (ox + 1) * a.ncx - 1);
-                xs_b[nxs] = cx;
-                xs_e[nxs] = end;
-                xs_o[nxs] = ox;
-                nxs++;
-                cx = end + 1;
-            }
-            const int n_items = (cy1 >= cy0) ? (cy1 - cy0 + 1) * nxs : 0;
+            int xs_b[3] = {0, 0, 0}, xs_e[3] = {0, 0, 0}, xs_o[3] = {0, 0, 0};
+            int ys_b[3] = {0, 0, 0}, ys_e[3] = {0, 0, 0}, ys_o[3] = {0, 0, 0};
+            const int nxs = cell_pieces(X0 - R, X1 + R, a.lx, a.ncx, a.inv_cell, a.wrap, xs_b, xs_e, xs_o);
+            const int nys = cell_pieces(Y0 - R, Y1 + R, a.ly, a.ncy, a.inv_cell, a.wrap, ys_b, ys_e, ys_o);
+            const int ny0 = nys > 0 ? ys_e[0] - ys_b[0] + 1 : 0, ny1 = nys > 1 ? ys_e[1] - ys_b[1] + 1 : 0;
+            const int ny2 = nys > 2 ? ys_e[2] - ys_b[2] + 1 : 0;
+            // items: (cell row of a y piece, x piece), rows in image order, then x pieces in image order
+            const int n_items = (ny0 + ny1 + ny2) * nxs;
             int nr = 0;
             unsigned run = 0;
             for (int base = 0; base < n_items && nr < kPotMaxRanges; base += 32) {
@@ -1168,13 +1189,25 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a)
                 unsigned b0 = 0, b1 = 0;
                 int img = 0;
                 if (it < n_items) {
-                    const int cy = cy0 + it / nxs, xi = it % nxs;
-                    const int oy = a.wrap ? floordiv_i(cy, a.ncy) : 0, cyw = cy - oy * a.ncy;
-                    const int cxw = xs_b[xi] - xs_o[xi] * a.ncx;
-                    const int64_t k0 = key_base + (int64_t)cyw * a.ncx + cxw;
+                    const int rr = it / nxs, xi = it % nxs;
+                    int cyw, oy;
+                    if (rr < ny0) {
+                        cyw = ys_b[0] + rr;
+                        oy = ys_o[0];
+                    } else if (rr < ny0 + ny1) {
+                        cyw = ys_b[1] + (rr - ny0);
+                        oy = ys_o[1];
+                    } else {
+                        cyw = ys_b[2] + (rr - ny0 - ny1);
+                        oy = ys_o[2];
+                    }
+                    const int pb = xi == 0 ? xs_b[0] : (xi == 1 ? xs_b[1] : xs_b[2]);
+                    const int pe = xi == 0 ? xs_e[0] : (xi == 1 ? xs_e[1] : xs_e[2]);
+                    const int po = xi == 0 ? xs_o[0] : (xi == 1 ? xs_o[1] : xs_o[2]);
+                    const int64_t k0 = key_base + (int64_t)cyw * a.ncx + pb;
                     b0 = a.seg[k0];
-                    b1 = a.seg[k0 + (xs_e[xi] - xs_b[xi]) + 1];
-                    img = (xs_o[xi] + 8) | ((oy + 8) << 8);
+                    b1 = a.seg[k0 + (pe - pb) + 1];
+                    img = (po + 8) | ((oy + 8) << 8);
                 }
                 const bool ok = b1 > b0;
                 const unsigned mask = __ballot_sync(0xffffffffu, ok);

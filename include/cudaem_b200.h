@@ -204,6 +204,14 @@ ms_status ms_set_graphs(ms_ctx* ctx, int enable);
  * operations (results agree to float rounding); the choice only changes speed.  No
  * reference counterpart (the reference's passes are cuFFT plans). */
 ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
+/* Order of the projected-potential work in the TEM, ED, CBED and thickness simulations:
+ * 0 (default) every slice's potential before the slice loop, on the context stream; 1 the
+ * potentials in 16-slice chunks, all but the first on a side stream while the slice passes of
+ * earlier slices run.  The results are identical.  The overlapped order competes with the
+ * slice passes for the SMs (a pass block needs the registers of half an SM), which makes a
+ * step slower than the serial order on some runs.  No reference counterpart (the reference
+ * generates each slice's potential just before its transmission, transmission_function.cuh:82-134). */
+ms_status ms_set_potential_overlap(ms_ctx* ctx, int enable);
 
 /* Per-kernel timing (no reference counterpart: the reference has no tracing).  While enabled,
  * every fused pass and potential launch is bracketed by CUDA events on the context stream;

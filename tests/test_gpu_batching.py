@@ -105,16 +105,16 @@ def test_stem_autotuned_batch(ctx):
 
 
 def test_potential_chunks_overlap_identical(ctx):
-    """Potentials computed in chunks on a side stream during the slice loop (the default) give the
-    same pattern as computing them all before the loop (the order per-launch profiling uses)."""
+    """Potentials computed in chunks on a side stream during the slice loop (the overlap switch)
+    give the same pattern as computing them all before the loop (the default)."""
     p, at = cases.cbed_small(n=128, cells=(2, 2, 12), nconf=3)   # about 48 slices: three chunks
     sim = cb.MulSimulator(ctx=ctx)
-    a = sim.executionCBED(p, at)
-    assert a.n_slices > 32
-    ctx.set_profiling(True)
+    ctx.set_potential_overlap(True)
     try:
-        b = sim.executionCBED(p, at)
+        a = sim.executionCBED(p, at)
     finally:
-        ctx.set_profiling(False)
+        ctx.set_potential_overlap(False)
+    assert a.n_slices > 32
+    b = sim.executionCBED(p, at)
     assert np.array_equal(a.image_intensity, b.image_intensity)
     assert rel_l2(a.image_intensity, orc.simulate_cbed(p, at)) < TOL

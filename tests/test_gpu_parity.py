@@ -33,6 +33,20 @@ def test_projected_potential(ctx, wrap, conf):
     assert rel_l2(V, Vo) < TOL_POT
 
 
+@pytest.mark.parametrize("cells,n,rmax,conf", [((5, 5, 4), 128, 3.0, 1), ((7, 5, 2), 256, 2.3, 0),
+                                               ((3, 4, 2), 128, 3.3, 1)])
+def test_projected_potential_periodic_images(ctx, cells, n, rmax, conf):
+    """Periodic wrap on boxes whose length is not a multiple of the atom-cell size (the cut-off):
+    the cell ranges of a pixel block are looked up per periodic image, so no image of an atom
+    within the cut-off of the box edges is missed."""
+    p, at = cases.hrtem_small(n=n, cells=cells, nconf=2, wrap=1)
+    p.pot_rmax = rmax
+    V = ctx.projected_potential(p, at, conf=conf)
+    Vo, _ = orc.potential(p, at, conf)
+    assert V.shape == Vo.shape
+    assert rel_l2(V, Vo) < TOL_POT
+
+
 @pytest.mark.parametrize("n", [128, 256, 512, 1024])
 def test_slice_loop_random_phases(ctx, n):
     p, _ = cases.stem_small(n=n)
