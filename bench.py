@@ -298,6 +298,15 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes (read + write) of one launch of a slice pass, from one ncu capture of the same launch
+# (8 waves of 1024^2 in flight, caches not flushed; profiles/slice_passes_1024_cbed_8waves.md):
+# keyed by (workload, kernel class, grid, waves per launch)
+DRAM_TRAFFIC = {
+    ("cbed", "col", 1024, 8): 58.424320e6 + 50.669824e6,
+    ("cbed", "row", 1024, 8): 130.682880e6 + 66.218752e6,
+}
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -408,12 +417,7 @@ def run_ours(args):
     avg_s = tot_ms / max(1, n_l) / 1e3
     achieved = algo / avg_s / 1e9
     peak, peak_kind = peaks()
-    hbm_traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            hbm_traffic = json.load(f).get(f"{args.config}:{dom}")
-    except Exception:
-        pass
+    hbm_traffic = DRAM_TRAFFIC.get((args.config, dom, p.nx, waves))
     line = {"metric": "probe*slice/s", "value": value, "unit": "probe*slice/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32-complex (fp64 phases)", "data": "synthetic",
