@@ -58,6 +58,15 @@ struct ms_ctx {
     // drains the stream so that no queued kernel still reads the old allocation.
     void* buf(const std::string& name, size_t bytes);
     void release_all();
+
+    // Free device memory as cudaMemGetInfo reports it.  The reading is kept until this context
+    // allocates or frees device memory: the query is a driver call that can wait behind other
+    // processes' queries of the device (a monitoring tool polling clocks, for one), and every
+    // simulation asks for it at its start, while the GPU is idle.
+    size_t free_mem();
+    void forget_free_mem() { free_known = false; }
+    bool free_known = false;
+    size_t free_seen = 0;
 };
 
 namespace msb {

@@ -31,10 +31,22 @@
                                  std::string(#x) + ": " + cudaGetErrorString(e_));                         \
     } while (0)
 
+size_t ms_ctx::free_mem()
+{
+    if (!free_known) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        free_seen = fr;
+        free_known = true;
+    }
+    return free_seen;
+}
+
 void* ms_ctx::buf(const std::string& name, size_t bytes)
 {
     Buf& b = bufs[name];
     if (b.p && b.bytes >= bytes) return b.p;
+    forget_free_mem();
     if (b.p) {
         cudaStreamSynchronize(stream);
         drop_graph();   // a captured graph may hold the old address
@@ -64,6 +76,7 @@ void ms_ctx::drop_graph()
 
 void ms_ctx::release_all()
 {
+    forget_free_mem();
     if (stream) cudaStreamSynchronize(stream);
     drop_graph();
     for (auto& kv : bufs)
@@ -175,6 +188,7 @@ const float2* twiddles(ms_ctx* c, int N)
         }
     void* p = nullptr;
     CK(cudaMalloc(&p, sizeof(float2) * 2 * N));
+    c->forget_free_mem();
     CK(cudaMemcpy(p, t.data(), sizeof(float2) * 2 * N, cudaMemcpyHostToDevice));
     c->twiddles[N] = p;
     return (const float2*)p;
@@ -322,6 +336,7 @@ Setup make_setup(ms_ctx* c, const ms_params& p)
             e[k] = make_float2((float)std::cos(a), (float)std::sin(a));
         }
         CK(cudaMalloc(&c->exptab, sizeof(float2) * 1024));
+        c->forget_free_mem();
         CK(cudaMemcpy(c->exptab, e.data(), sizeof(float2) * 1024, cudaMemcpyHostToDevice));
     }
     s.exptab = (const float2*)c->exptab;
@@ -690,11 +705,9 @@ struct Timer {
 };
 
 // free device memory budget for the potential store
-size_t free_budget()
+size_t free_budget(ms_ctx* c)
 {
-    size_t fr = 0, tot = 0;
-    cudaMemGetInfo(&fr, &tot);
-    return (size_t)(fr * 0.6);
+    return (size_t)(c->free_mem() * 0.6);
 }
 
 void copy_out(ms_ctx* c, float* dst, const float* src, int64_t n, int on_dev)
@@ -761,7 +774,7 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
     int S_est = estimate_slices(p, a);
     size_t per_conf = (size_t)S_est * N * 8 + (size_t)N * 8 * 2 + (size_t)N * 4 + (size_t)a.n * 40 +
                       fine_bytes_per_conf(p, a);
-    int gsize = (int)std::max<size_t>(1, std::min<size_t>(cs.confs.size(), free_budget() / per_conf));
+    int gsize = (int)std::max<size_t>(1, std::min<size_t>(cs.confs.size(), free_budget(c) / per_conf));
 
     double* acc = (double*)c->buf("acc0", sizeof(double) * N);
     double* acc_im = full ? (double*)c->buf("acc1", sizeof(double) * N) : nullptr;
@@ -901,10 +914,9 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
 // ---------------------------------------------------------------------------
 namespace {
 // Largest probe batch the memory budget allows (the waves take at most a quarter of free memory).
-int batch_cap(int64_t N)
+int batch_cap(ms_ctx* c, int64_t N)
 {
-    size_t fr = 0, tot = 0;
-    cudaMemGetInfo(&fr, &tot);
+    const size_t fr = c->free_mem();
     int64_t cap = (int64_t)(fr * 0.25 / (double)(N * 8));
     return (int)std::min<int64_t>(256, std::max<int64_t>(1, cap));
 }
@@ -1055,7 +1067,7 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
     double* img = (double*)c->buf("stem_acc", sizeof(double) * ndet * npos);
     CK(cudaMemsetAsync(img, 0, sizeof(double) * ndet * npos, st));
     const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
-    const int cap = plain ? 1 : (p.probe_batch > 0 ? std::min(p.probe_batch, npos) : batch_cap(N));
+    const int cap = plain ? 1 : (p.probe_batch > 0 ? std::min(p.probe_batch, npos) : batch_cap(c, N));
     int B = plain ? 1 : std::min(cap, npos);
     bool tuned = plain || p.probe_batch > 0;
     std::vector<WaveInfo> wv((size_t)npos);
@@ -1391,7 +1403,7 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
     // checkpoints must fit the memory budget
     const size_t per_wave = (size_t)N * 8 * (2 + 2 * (size_t)k + (size_t)(nseg - 1));
     int B = p.probe_batch > 0 ? p.probe_batch : 256;
-    B = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, free_budget() / per_wave));
+    B = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, free_budget(c) / per_wave));
     B = std::min(B, np);
     const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>(64, N / 4096));
     const int tiles = col_tiles(p.ny, p.nx);
@@ -1605,7 +1617,7 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
     }
     int r0 = 0;
     while (r0 < n) {
-        size_t budget = free_budget(), used = 0;
+        size_t budget = free_budget(c), used = 0;
         int r1 = r0;
         while (r1 < n && (r1 == r0 || used + need[r1] <= budget)) used += need[r1++];
         // one arena, cached in the context like every other buffer, holds the round's per-instance
@@ -1784,6 +1796,7 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
                 if (it != c->bufs.end()) {
                     cudaFree(it->second.p);
                     c->bufs.erase(it);
+                    c->forget_free_mem();
                 }
             }
         }
