@@ -602,7 +602,8 @@ PotArgs pot_args(const ms_params& p, const Setup& s, const AtomsDev& A, const Sp
     return a;
 }
 
-// Potential chunks computed on a side stream (see sim_tem_like).
+// Potential chunks computed on a side stream when the context's potential overlap is on (see
+// sim_tem_like); otherwise all slices in one launch before the slice loop.
 constexpr int kPotChunk = 16;
 struct PotChunks {
     std::vector<cudaEvent_t> ev;   // ev[k]: slices [k kPotChunk, (k+1) kPotChunk) are written
@@ -659,8 +660,8 @@ PotChunks launch_potential_chunks(ms_ctx* c, PotArgs a, int n_conf, int S)
 }
 
 // The potential kernel writing the transmission function t = exp(i V) (complex) instead of V:
-// the slice passes then read t, and the exponential is formed once per pixel and slice, on the
-// potential kernel's side stream, instead of in the latency-bound row pass.
+// the slice passes then read t, and the exponential is formed once per pixel and slice in the
+// potential kernel, instead of once per wave in the latency-bound row pass.
 PotArgs with_transmission(PotArgs a, float2* T, const Setup& s)
 {
     a.T = T;
