@@ -1123,7 +1123,9 @@ __device__ __forceinline__ int cell_pieces(float lo, float hi, float L, int nc, 
     return n;
 }
 
-template <bool FINE>
+// WRAP is the periodic wrap of the specimen (a.wrap), a template argument so that the
+// non-periodic kernel carries none of the per-image lookup code
+template <bool FINE, bool WRAP>
 __global__ void __launch_bounds__(kPotThreads, 6) k_potential(PotArgs a)
 {
     extern __shared__ __align__(16) unsigned char psm[];
@@ -1176,8 +1178,8 @@ __global__ void __launch_bounds__(kPotThreads, 6) k_potential(PotArgs a)
             const int64_t key_base = ((int64_t)conf * (a.S_cap + 1) + sl) * a.ncx * a.ncy;
             int xs_b[3] = {0, 0, 0}, xs_e[3] = {0, 0, 0}, xs_o[3] = {0, 0, 0};
             int ys_b[3] = {0, 0, 0}, ys_e[3] = {0, 0, 0}, ys_o[3] = {0, 0, 0};
-            const int nxs = cell_pieces(X0 - R, X1 + R, a.lx, a.ncx, a.inv_cell, a.wrap, xs_b, xs_e, xs_o);
-            const int nys = cell_pieces(Y0 - R, Y1 + R, a.ly, a.ncy, a.inv_cell, a.wrap, ys_b, ys_e, ys_o);
+            const int nxs = cell_pieces(X0 - R, X1 + R, a.lx, a.ncx, a.inv_cell, WRAP, xs_b, xs_e, xs_o);
+            const int nys = cell_pieces(Y0 - R, Y1 + R, a.ly, a.ncy, a.inv_cell, WRAP, ys_b, ys_e, ys_o);
             const int ny0 = nys > 0 ? ys_e[0] - ys_b[0] + 1 : 0, ny1 = nys > 1 ? ys_e[1] - ys_b[1] + 1 : 0;
             const int ny2 = nys > 2 ? ys_e[2] - ys_b[2] + 1 : 0;
             // items: (cell row of a y piece, x piece), rows in image order, then x pieces in image order
@@ -1357,13 +1359,17 @@ void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st)
     if (a.nslice <= 0 || n_conf <= 0) return;
     dim3 grid((unsigned)((a.nx / kPotTX) * (a.ny / kPotTY)), (unsigned)a.nslice, (unsigned)n_conf);
     size_t sm = sizeof(ElemTable) * a.n_elem + sizeof(float4) * kPotThreads;
+    if (a.pair_coef) sm += sizeof(unsigned) * kPotThreads;
+    auto go = [&](auto kern) {
+        smem_attr(kern, sm);
+        kern<<<grid, kPotThreads, sm, st>>>(a);
+    };
     if (a.pair_coef) {
-        sm += sizeof(unsigned) * kPotThreads;
-        smem_attr(k_potential<true>, sm);
-        k_potential<true><<<grid, kPotThreads, sm, st>>>(a);
+        if (a.wrap) go(k_potential<true, true>);
+        else go(k_potential<true, false>);
     } else {
-        smem_attr(k_potential<false>, sm);
-        k_potential<false><<<grid, kPotThreads, sm, st>>>(a);
+        if (a.wrap) go(k_potential<false, true>);
+        else go(k_potential<false, false>);
     }
     count_launch();
     check_launch("potential");
