@@ -160,3 +160,10 @@ def test_no_device_is_reported():
         pytest.skip("a GPU is present")
     h = C.c_void_p()
     assert cb.lib().ms_create(C.byref(h), 0) == abi.MS_ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("name", ["ms_set_graphs", "ms_set_pass_kernels", "ms_set_potential_overlap",
+                                  "ms_set_profiling"])
+def test_context_switches_reject_a_null_context(name):
+    """The context switches check their handle before touching any device state."""
+    assert getattr(cb.lib(), name)(None, 1) == abi.MS_ERR_INVALID_ARG
