@@ -1126,7 +1126,7 @@ __device__ __forceinline__ int cell_pieces(float lo, float hi, float L, int nc, 
 // WRAP is the periodic wrap of the specimen (a.wrap), a template argument so that the
 // non-periodic kernel carries none of the per-image lookup code
 template <bool FINE, bool WRAP>
-__global__ void __launch_bounds__(kPotThreads, 6) k_potential(PotArgs a)
+__global__ void __launch_bounds__(kPotThreads, 8) k_potential(PotArgs a)
 {
     extern __shared__ __align__(16) unsigned char psm[];
     ElemTable* el = reinterpret_cast<ElemTable*>(psm);
