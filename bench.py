@@ -299,7 +299,7 @@ def run_reference(args):
 
 
 # DRAM bytes (read + write) of one launch of a slice pass, from one ncu capture of the same launch
-# (8 waves of 1024^2 in flight, caches not flushed; profiles/slice_passes_1024_cbed_8waves.md):
+# (8 waves of 1024^2 in flight, caches not flushed, after the same command ran without ncu):
 # keyed by (workload, kernel class, grid, waves per launch)
 DRAM_TRAFFIC = {
     ("cbed", "col", 1024, 8): 58.424320e6 + 50.669824e6,
