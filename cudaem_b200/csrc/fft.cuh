@@ -65,6 +65,20 @@ __device__ __forceinline__ float2 tw_apply(float2 d, int m)
 {
     if (m == 0) return d;
     if (m == 16) return DIR < 0 ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);
+    if (m == 8 || m == 24) {
+        // W_64^8 = (1 - i)/sqrt2 and W_64^24 = (-1 - i)/sqrt2 (their conjugates for DIR > 0): a sum
+        // and a difference of the two parts, each scaled by 1/sqrt2 carried as hi + lo
+        const float hs = c_tw64[8].x, ls = c_tw64_lo[8].x;
+        float re, im;
+        if (DIR < 0) {
+            re = (m == 8) ? d.x + d.y : d.y - d.x;
+            im = (m == 8) ? d.y - d.x : -(d.x + d.y);
+        } else {
+            re = (m == 8) ? d.x - d.y : -(d.x + d.y);
+            im = (m == 8) ? d.x + d.y : d.x - d.y;
+        }
+        return make_float2(fmaf(re, hs, re * ls), fmaf(im, hs, im * ls));
+    }
     return DIR < 0 ? cmul_split(d, c_tw64[m], c_tw64_lo[m]) : cmulc_split(d, c_tw64[m], c_tw64_lo[m]);
 }
 
