@@ -302,8 +302,8 @@ def run_reference(args):
 # (8 waves of 1024^2 in flight, caches not flushed, after the same command ran without ncu):
 # keyed by (workload, kernel class, grid, waves per launch)
 DRAM_TRAFFIC = {
-    ("cbed", "col", 1024, 8): 58.424320e6 + 50.669824e6,
-    ("cbed", "row", 1024, 8): 130.682880e6 + 66.218752e6,
+    ("cbed", "col", 1024, 8): 57.831936e6 + 50.721792e6,
+    ("cbed", "row", 1024, 8): 130.415360e6 + 65.834752e6,
 }
 
 
