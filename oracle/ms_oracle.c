@@ -921,6 +921,15 @@ static void or_incident(const ms_params* p, const or_sim* s, double px, double p
         or_lens_init(&p->cond_lens, s->lambda, z_init, &L);
         or_probe_k(s, &L, px, py, w);
         or_fft2c(w, s->nx, s->ny, +1);
+    } else if (iw == MS_IW_PLANE_TILTED) {
+        /* Incident_Wave::apply_beam_tilt (incident_wave.cuh:72-78) on the plane wave: exp_r_factor_2d
+           (device_kernels.cuh:519-533) with (2 pi gx_0, 2 pi gy_0), R = (i dx - lx/2, j dy - ly/2) */
+        for (int iy = 0; iy < s->ny; iy++)
+            for (int ix = 0; ix < s->nx; ix++) {
+                double rx = ix * s->dx - 0.5 * s->lx, ry = iy * s->dy - 0.5 * s->ly;
+                double ph = 2.0 * OR_PI * (s->g0x * rx + s->g0y * ry);
+                w[(size_t)iy * s->nx + ix] = cos(ph) + I * sin(ph);
+            }
     } else {
         for (long k = 0; k < s->N; k++) w[k] = 1.0;
     }
@@ -1147,6 +1156,56 @@ static int or_tem_like(const ms_params* p, const ms_atoms* a, double* img, doubl
     }
     free(es);
     free(wv);
+    free(P);
+    free(Vt);
+    return 0;
+}
+
+/* Defocus series (apply_CTF_kernel_batch, device_kernels.cuh:469-503): every exit wave imaged
+   through the coherent objective lens with chi + defocus-term(df_i) g^2, i.e. the lens at
+   C10 + df[i]; images (or complex fields) summed over configurations, [nd][ny][nx]. */
+int or_simulate_tem_series(const ms_params* p, const ms_atoms* a, int nd, const double* df, double* img, double* re,
+                           double* im)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    int c0, c1;
+    double w;
+    or_confs(p, &c0, &c1, &w);
+    int full = p->data_record == MS_RECORD_WAVE;
+    size_t NN = (size_t)s.N * nd;
+    if (img) memset(img, 0, sizeof(double) * NN);
+    if (re) memset(re, 0, sizeof(double) * NN);
+    if (im) memset(im, 0, sizeof(double) * NN);
+    cplx* wv = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    cplx* tmp = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)s.N);
+    double* Vt = (double*)malloc(sizeof(double) * (size_t)s.N);
+    or_propagator(p, &s, P);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    for (int c = c0; c <= c1; c++) {
+        or_spec sp;
+        or_spec_build(p, a, c, &sp);
+        or_incident(p, &s, p->iw_x, p->iw_y, sp.z_init, wv);
+        or_multislice(&s, wv, NULL, sp.ns, P, p, a, &sp, es, Vt);
+        for (int i = 0; i < nd; i++) {
+            or_lens L;
+            or_lens_init(&p->obj_lens, s.lambda, df[i], &L);
+            or_ctf_image(p, &s, &L, 0.0, 0.0, 0, 1.0, wv, tmp);
+            size_t o = (size_t)i * s.N;
+            for (long k = 0; k < s.N; k++) {
+                if (full) {
+                    re[o + k] += w * creal(tmp[k]);
+                    im[o + k] += w * cimag(tmp[k]);
+                } else
+                    img[o + k] += w * (creal(tmp[k]) * creal(tmp[k]) + cimag(tmp[k]) * cimag(tmp[k]));
+            }
+        }
+        or_spec_free(&sp);
+    }
+    free(es);
+    free(wv);
+    free(tmp);
     free(P);
     free(Vt);
     return 0;
@@ -1445,6 +1504,114 @@ int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_
     *loss = Ltot;
     *dL_dC10 = g10;
     *dL_dC30 = g30;
+    free(T);
+    free(P);
+    return 0;
+}
+
+/* Central finite differences of the loss of or_stem_forward_potential.  Every task (one pixel
+   and one sign, or one lens coefficient and one sign) runs single-threaded on its own wave;
+   a pixel task restarts each probe from the unperturbed wave stored every FD_CK slices before
+   the perturbed slice, so only the slices from that store on are recomputed. */
+#define FD_CK 8
+static double or_fd_loss_from(const ms_params* p, const or_sim* s, const cplx* T, const cplx* P, int S, int s0,
+                              int sp, long kp, double dv, const cplx* w0, const float* target, int ip, cplx* w)
+{
+    long N = s->N;
+    memcpy(w, w0, sizeof(cplx) * (size_t)N);
+    for (int i = s0; i < S; i++) {
+        const cplx* t = T + (size_t)i * N;
+        for (long k = 0; k < N; k++) w[k] *= t[k];
+        if (i == sp) w[kp] *= cos(dv) + I * sin(dv); /* exp(i (V + dv)) = exp(i V) exp(i dv) */
+        or_fft2c(w, s->nx, s->ny, -1);
+        if (i < S - 1) {
+            for (long k = 0; k < N; k++) w[k] *= P[k];
+            or_fft2c(w, s->nx, s->ny, +1);
+        }
+    }
+    double Id[MS_MAX_DET], L = 0.0;
+    or_detect(p, s, w, Id);
+    for (int d = 0; d < p->n_det; d++) {
+        double r = Id[d] - (double)target[(size_t)ip * p->n_det + d];
+        L += r * r;
+    }
+    return L;
+}
+
+int or_stem_loss_fd(const ms_params* p, const float* V, int n_slices, double z_init, const double* probe_xy,
+                    int n_probe, const float* target, int n_pix, const int64_t* idx, const double* h,
+                    double h10, double h30, double* fd_pix, double* fd_c10, double* fd_c30)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    long N = s.N;
+    int S = n_slices;
+    int nck = (S + FD_CK - 1) / FD_CK;
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+    or_propagator(p, &s, P);
+    cplx* T = (cplx*)malloc(sizeof(cplx) * (size_t)N * S);
+    for (int i = 0; i < S; i++) or_exp_phase(V + (size_t)i * N, N, T + (size_t)i * N);
+    /* unperturbed waves in front of slices 0, FD_CK, 2 FD_CK, ... per probe */
+    cplx* ck = (cplx*)malloc(sizeof(cplx) * (size_t)N * nck * n_probe);
+    int nth = or_get_threads();
+#pragma omp parallel for num_threads(nth) schedule(dynamic, 1)
+    for (int ip = 0; ip < n_probe; ip++) {
+        ms_params q = *p;
+        q.iw_type = MS_IW_CONVERGENT;
+        cplx* w = ck + (size_t)ip * nck * N;
+        or_incident(&q, &s, probe_xy[2 * ip], probe_xy[2 * ip + 1], z_init, w);
+        for (int c = 1; c < nck; c++) {
+            cplx* nx = w + (size_t)c * N;
+            memcpy(nx, w + (size_t)(c - 1) * N, sizeof(cplx) * (size_t)N);
+            for (int i = (c - 1) * FD_CK; i < c * FD_CK; i++) {
+                const cplx* t = T + (size_t)i * N;
+                for (long k = 0; k < N; k++) nx[k] *= t[k];
+                or_fft2c(nx, s.nx, s.ny, -1);
+                for (long k = 0; k < N; k++) nx[k] *= P[k];
+                or_fft2c(nx, s.nx, s.ny, +1);
+            }
+        }
+    }
+    int ntask = 2 * n_pix + 4;
+    double* Ls = (double*)calloc((size_t)ntask, sizeof(double));
+#pragma omp parallel num_threads(nth)
+    {
+        cplx* w = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+        cplx* w0 = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+#pragma omp for schedule(dynamic, 1)
+        for (int task = 0; task < ntask; task++) {
+            double L = 0.0;
+            if (task < 2 * n_pix) {
+                int j = task / 2;
+                double dv = (task % 2 == 0) ? h[j] : -h[j];
+                int sp = (int)(idx[j] / N);
+                long kp = (long)(idx[j] % N);
+                int c = sp / FD_CK;
+                for (int ip = 0; ip < n_probe; ip++)
+                    L += or_fd_loss_from(p, &s, T, P, S, c * FD_CK, sp, kp, dv, ck + ((size_t)ip * nck + c) * N,
+                                         target, ip, w);
+            } else {
+                int lt = task - 2 * n_pix;
+                ms_params q = *p;
+                q.iw_type = MS_IW_CONVERGENT;
+                double sg = (lt % 2 == 0) ? 1.0 : -1.0;
+                if (lt < 2) q.cond_lens.c10 += sg * h10;
+                else q.cond_lens.c30 += sg * h30;
+                for (int ip = 0; ip < n_probe; ip++) {
+                    or_incident(&q, &s, probe_xy[2 * ip], probe_xy[2 * ip + 1], z_init, w0);
+                    L += or_fd_loss_from(p, &s, T, P, S, 0, -1, 0, 0.0, w0, target, ip, w);
+                }
+            }
+            Ls[task] = L;
+        }
+        free(w);
+        free(w0);
+    }
+    for (int j = 0; j < n_pix; j++) fd_pix[j] = (Ls[2 * j] - Ls[2 * j + 1]) / (2.0 * h[j]);
+    *fd_c10 = (Ls[2 * n_pix] - Ls[2 * n_pix + 1]) / (2.0 * h10);
+    *fd_c30 = (Ls[2 * n_pix + 2] - Ls[2 * n_pix + 3]) / (2.0 * h30);
+    free(Ls);
+    free(ck);
     free(T);
     free(P);
     return 0;

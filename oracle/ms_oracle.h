@@ -56,12 +56,22 @@ int or_simulate_stem(const ms_params* p, const ms_atoms* a, double* stem);
 int or_simulate_thickness(const ms_params* p, const ms_atoms* a, double* frames, int64_t cap,
                           int* n_frames);
 
+/* HRTEM defocus series: images at objective C10 + df[i], [nd][ny][nx] */
+int or_simulate_tem_series(const ms_params* p, const ms_atoms* a, int nd, const double* df, double* img, double* re,
+                           double* im);
+
 /* raw STEM forward / adjoint on caller phase arrays V[n_slices][ny][nx] */
 int or_stem_forward_potential(const ms_params* p, const float* V, int n_slices, double z_init,
                               const double* probe_xy, int n_probe, double* I);
 int or_stem_backward(const ms_params* p, const float* V, int n_slices, double z_init,
                      const double* probe_xy, int n_probe, const float* target, double* loss,
                      double* dL_dV, double* dL_dC10, double* dL_dC30);
+/* central differences of the same loss L = sum (I - target)^2 of the FP64 forward: with respect to
+   single potential pixels (flat index idx[j] into V, step h[j]) and to the condenser C10 and C30
+   (steps h10, h30); fd_pix[j] = (L(V + h e_j) - L(V - h e_j)) / (2 h[j]) */
+int or_stem_loss_fd(const ms_params* p, const float* V, int n_slices, double z_init, const double* probe_xy,
+                    int n_probe, const float* target, int n_pix, const int64_t* idx, const double* h,
+                    double h10, double h30, double* fd_pix, double* fd_c10, double* fd_c30);
 
 /* operator-level entry points, checked against the reference's own kernels (ref_shim/):
    propagator table, k-space probe, CTF / PCTF (no inverse FFT), detector sums, and the slice

@@ -76,10 +76,13 @@ def lib() -> C.CDLL:
             "or_fft2": (None, [P(d), i, i, i]),
             "or_simulate_tem": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), P(d), P(d)]),
             "or_simulate_cbed": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), P(d), P(d)]),
+            "or_simulate_tem_series": (i, [P(abi.ms_params), P(abi.ms_atoms), i, P(d), P(d), P(d), P(d)]),
             "or_simulate_stem": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d)]),
             "or_simulate_thickness": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), C.c_int64, P(i)]),
             "or_stem_forward_potential": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(d)]),
             "or_stem_backward": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(f), P(d), P(d), P(d), P(d)]),
+            "or_stem_loss_fd": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(f), i, P(C.c_int64), P(d), d, d,
+                                    P(d), P(d), P(d)]),
             "or_gauss_hermite": (None, [i, P(d), P(d)]),
             "or_gauss_legendre_half": (None, [i, P(d), P(d)]),
             "or_fine_spline_table": (i, [P(abi.ms_params), i, d, d, P(d), P(d), P(d), P(d), P(d)]),
@@ -198,6 +201,19 @@ def simulate_tem(params, atoms):
     return img if img is not None else (re, im)
 
 
+def simulate_tem_series(params, atoms, defocus):
+    df = np.ascontiguousarray(defocus, np.float64).ravel()
+    n = (df.size, params.ny, params.nx)
+    p, a = params.c(), atoms.c()
+    if params.data_record == 1:
+        re, im = np.empty(n), np.empty(n)
+        lib().or_simulate_tem_series(C.byref(p), C.byref(a), df.size, _d(df), None, _d(re), _d(im))
+        return re, im
+    img = np.empty(n)
+    lib().or_simulate_tem_series(C.byref(p), C.byref(a), df.size, _d(df), _d(img), None, None)
+    return img
+
+
 def simulate_cbed(params, atoms):
     img, re, im = _img_outputs(params)
     p, a = params.c(), atoms.c()
@@ -242,6 +258,24 @@ def stem_backward(params, V, z_init, xy, target):
     lib().or_stem_backward(C.byref(p), _f(V), V.shape[0], z_init, _d(xy), xy.shape[0], _f(T), C.byref(loss),
                            _d(gV), C.byref(g10), C.byref(g30))
     return loss.value, gV, g10.value, g30.value
+
+
+def stem_loss_fd(params, V, z_init, xy, target, idx, h, h10, h30):
+    """Central differences of L = sum (I - target)^2 (FP64 forward) at the flat pixel indices
+    `idx` of V (steps h) and for the condenser C10 and C30 (steps h10, h30)."""
+    V = np.ascontiguousarray(V, np.float32)
+    xy = np.ascontiguousarray(xy, np.float64).reshape(-1, 2)
+    T = np.ascontiguousarray(target, np.float32)
+    idx = np.ascontiguousarray(idx, np.int64)
+    h = np.ascontiguousarray(h, np.float64)
+    fd = np.empty(idx.size)
+    f10, f30 = C.c_double(), C.c_double()
+    p = params.c()
+    rc = lib().or_stem_loss_fd(C.byref(p), _f(V), V.shape[0], z_init, _d(xy), xy.shape[0], _f(T), idx.size,
+                               idx.ctypes.data_as(C.POINTER(C.c_int64)), _d(h), h10, h30, _d(fd), C.byref(f10),
+                               C.byref(f30))
+    assert rc == 0
+    return fd, f10.value, f30.value
 
 
 def gauss_hermite(n: int):

@@ -120,3 +120,32 @@ def test_backward_differentiable_stem_shape(ctx):
     assert rel_l2(gV, gVo) < 1e-3
     assert abs(g10 - g10o) / abs(g10o) < 1e-3
     assert abs(g30 - g30o) / abs(g30o) < 1e-3
+
+
+def test_backward_finite_differences_differentiable_stem_shape(ctx):
+    """The differentiable-STEM check at its own shape: SrTiO3 10x10x40 cells, 512^2, 80 slices,
+    checkpoints every 8, targets simulated from potentials perturbed by Gaussian noise at 1 % of
+    |V|.  GPU gradients against central differences (h = 1e-3 relative) of the FP64 forward loss
+    on 64 potential pixels drawn uniformly over all 80 x 512^2, and on C10 and Cs.  Four of the
+    workload's 16 probes, so that the 132 FP64 forward evaluations finish in about a minute."""
+    from cudaem_b200 import workloads as wl
+    p, at, xy = wl.adjoint_sto(n_probe=4)
+    V = ctx.projected_potential(p, at, conf=0)
+    assert V.shape == (80, 512, 512) and p.ckpt_interval == 8
+    z0 = 0.5 * p.dz
+    rng = np.random.default_rng(11)
+    Vt = (V + 0.01 * np.abs(V) * rng.standard_normal(V.shape)).astype(np.float32)
+    T = orc.stem_forward_potential(p, Vt, z0, xy).astype(np.float32)
+    loss, gV, g10, g30 = ctx.stem_backward(p, V, z0, xy, T)
+    idx = rng.choice(V.size, size=64, replace=False)
+    h = 1e-3 * np.maximum(np.abs(V.ravel()[idx]).astype(np.float64), 1e-3)
+    fd, f10, f30 = orc.stem_loss_fd(p, V, z0, xy, T, idx, h, 1e-3 * abs(p.cond_lens.c10),
+                                    1e-3 * abs(p.cond_lens.c30))
+    an = gV.ravel()[idx].astype(np.float64)
+    e_pix = rel_l2(an, fd)
+    e10, e30 = abs(g10 - f10) / abs(f10), abs(g30 - f30) / abs(f30)
+    print(f"differentiable STEM 512^2 x 80 slices: dL/dV on 64 random pixels rel L2 {e_pix:.2e}, "
+          f"dL/dC10 {e10:.2e}, dL/dCs {e30:.2e}")
+    assert e_pix < TOL_GRAD
+    assert e10 < TOL_GRAD
+    assert e30 < TOL_GRAD

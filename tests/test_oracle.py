@@ -12,6 +12,7 @@ import cases  # noqa: E402
 import numpy_twin as tw  # noqa: E402
 from conftest import rel_l2  # noqa: E402
 from oracle import oracle as orc  # noqa: E402
+import cudaem_b200 as cb  # noqa: E402
 
 
 # relativistic wavelength (A) and interaction constant (rad/(V A)): textbook values
@@ -212,3 +213,34 @@ def test_fine_slicing_integrates_the_projection():
     x, w = np.empty(64), np.empty(64)
     L.or_gauss_legendre_half(64, d(x), d(w))
     assert abs(w.sum() - 1) < 1e-13 and abs(np.dot(w, x ** 2) - 1 / 12) < 1e-14 and abs(np.dot(w, x ** 4) - 1 / 80) < 1e-14
+
+
+def test_defocus_series_equals_shifted_lens():
+    """The oracle's defocus series (apply_CTF_kernel_batch restated) equals single HRTEM images with
+    the objective lens moved to C10 + df."""
+    p, at = cases.hrtem_small(nconf=2)
+    dfs = [-80.0, 0.0, 55.0]
+    ser = orc.simulate_tem_series(p, at, dfs)
+    for i, df in enumerate(dfs):
+        q = p.copy()
+        q.obj_lens.c10 = p.obj_lens.c10 + df
+        assert rel_l2(ser[i], orc.simulate_tem(q, at)) < 1e-12
+
+
+def test_tilted_plane_wave_vacuum():
+    """A tilted plane wave exp(2 pi i g0.(r - L/2)) whose g0 lies on the frequency grid stays a single
+    Fourier component through vacuum slices under the tilted propagator: the ED pattern of an empty
+    specimen is one bright pixel at g0."""
+    from cudaem_b200 import _abi as abi
+    p, at = cases.ed_small(nconf=1)
+    lam, _, _ = orc.physics(p.E0)
+    m = 3
+    p.phi = 0.0
+    p.theta = float(np.arcsin(m / p.lx * lam))
+    p.iw_type = abi.MS_IW_PLANE_TILTED
+    far = cb.Atoms(Z=np.array([8], np.int32), x=np.array([0.5], np.float32), y=np.array([0.5], np.float32),
+                   z=np.array([0.0], np.float32), sigma=np.zeros(1, np.float32), occ=np.zeros(1, np.float32))
+    img = orc.simulate_tem(p, far)
+    peak = np.unravel_index(np.argmax(img), img.shape)
+    assert peak == (p.ny // 2, p.nx // 2 + m)
+    assert img[peak] / img.sum() > 1 - 1e-9
