@@ -382,6 +382,26 @@ class MulSimulator:
         self.ctx.check(lib().ms_simulate_tem(self.ctx.handle, C.byref(p), C.byref(a), C.byref(co)))
         return self._finish(o, co)
 
+    def executionTEMDefocusSeries(self, params: MultisliceParams, atoms: Atoms,
+                                  defocus: Sequence[float]) -> OutputMultiData:
+        """HRTEM images at objective-lens defocus C10 + defocus[i] from one multislice run
+        (ms_simulate_tem_defocus_series); the image arrays are [n_defocus][ny][nx]."""
+        df = np.ascontiguousarray(defocus, np.float64).ravel()
+        shape = (df.size, params.ny, params.nx)
+        if params.data_record == abi.MS_RECORD_WAVE:
+            o = OutputMultiData(image_real=np.empty(shape, np.float32), image_imag=np.empty(shape, np.float32))
+        else:
+            o = OutputMultiData(image_intensity=np.empty(shape, np.float32))
+        co = abi.ms_output()
+        for name in ("image_intensity", "image_real", "image_imag"):
+            arr = getattr(o, name)
+            if arr is not None:
+                setattr(co, name, arr.ctypes.data_as(C.POINTER(C.c_float)))
+        p, a = params.c(), atoms.c()
+        self.ctx.check(lib().ms_simulate_tem_defocus_series(self.ctx.handle, C.byref(p), C.byref(a), df.size,
+                                                           df.ctypes.data_as(C.POINTER(C.c_double)), C.byref(co)))
+        return self._finish(o, co)
+
     def executionCBED(self, params: MultisliceParams, atoms: Atoms) -> OutputMultiData:
         o, co = self._out(params, "image")
         p, a = params.c(), atoms.c()

@@ -21,13 +21,13 @@ STATUS_NAMES = {0: "MS_OK", 1: "MS_ERR_INVALID_ARG", 2: "MS_ERR_UNSUPPORTED", 3:
 
 MS_SIM_HRTEM, MS_SIM_ED, MS_SIM_CBED, MS_SIM_STEM = 1, 2, 3, 4
 MS_PHONON_STILL, MS_PHONON_FROZEN = 1, 3
-MS_IW_PLANE, MS_IW_CONVERGENT = 1, 2
+MS_IW_PLANE, MS_IW_CONVERGENT, MS_IW_PLANE_TILTED = 1, 2, 3
 (MS_POT_DOYLE_0_4, MS_POT_PENG_0_4, MS_POT_PENG_0_12, MS_POT_KIRKLAND_0_12, MS_POT_WEICKENMEIER_0_12,
  MS_POT_LOBATO_0_12, MS_POT_MOLIERE) = range(1, 8)
 MS_ILLUM_COHERENT, MS_ILLUM_PARTIAL, MS_ILLUM_TCC = 1, 2, 3
 MS_TSI_TEMPORAL_SPATIAL, MS_TSI_TEMPORAL, MS_TSI_SPATIAL, MS_TSI_COHERENT = 1, 2, 3, 4
 MS_RECORD_INTENSITY, MS_RECORD_WAVE = 0, 1
-MS_EXEC_BATCHED, MS_EXEC_PLAIN = 0, 1
+MS_EXEC_BATCHED, MS_EXEC_PLAIN, MS_EXEC_GENERAL = 0, 1, 2
 MS_BORDER_MIN, MS_BORDER_MAX, MS_BORDER_MIDDLE = 0, 1, 2
 
 
@@ -128,6 +128,8 @@ PROTOTYPES = {
     "ms_profile_get": (C.c_int, [C.c_void_p, C.c_char_p, _P(C.c_int64), _P(C.c_double)]),
     "ms_physics": (C.c_int, [C.c_double, _P(C.c_double), _P(C.c_double), _P(C.c_double)]),
     "ms_simulate_tem": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), _P(ms_output)]),
+    "ms_simulate_tem_defocus_series": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), C.c_int,
+                                                 _P(C.c_double), _P(ms_output)]),
     "ms_simulate_cbed": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), _P(ms_output)]),
     "ms_simulate_stem": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), _P(ms_output)]),
     "ms_simulate_thickness": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), _P(ms_output)]),

@@ -22,7 +22,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "engine.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "passes_128.cu", "passes_256.cu", "passes_512.cu", "passes_1024.cu", "passes_2048.cu",
+              "engine.cu", "noalloc.cu"]
 CPP_SOURCES = ["host.cpp", "abi.cpp"]
 
 

@@ -18,19 +18,21 @@ thread_local std::string g_noctx_err;
 template <class F>
 ms_status guarded(ms_ctx* c, F&& f)
 {
+    // calls without a context keep their message per host thread (ms_last_error(NULL)); a success
+    // clears it like a context's
+    std::string& err = c ? c->err : g_noctx_err;
     try {
         f();
-        if (c) c->err.clear();
+        err.clear();
         return MS_OK;
     } catch (const msb::MsError& e) {
-        if (c) c->err = e.what();
-        else g_noctx_err = e.what();
+        err = e.what();
         return e.st;
     } catch (const std::bad_alloc&) {
-        if (c) c->err = "host allocation failed";
+        err = "host allocation failed";
         return MS_ERR_OUT_OF_MEMORY;
     } catch (const std::exception& e) {
-        if (c) c->err = e.what();
+        err = e.what();
         return MS_ERR_INTERNAL;
     }
 }
@@ -214,6 +216,21 @@ ms_status ms_simulate_tem(ms_ctx* c, const ms_params* p, const ms_atoms* a, ms_o
         MS_REQUIRE(p->simulation_type == MS_SIM_HRTEM || p->simulation_type == MS_SIM_ED, MS_ERR_INVALID_ARG,
                    "ms_simulate_tem runs HRTEM or ED");
         msb::sim_tem_like(c, *p, *a, out, false);
+    });
+}
+
+ms_status ms_simulate_tem_defocus_series(ms_ctx* c, const ms_params* p, const ms_atoms* a, int n_defocus,
+                                         const double* defocus, ms_output* out)
+{
+    if (!c) return MS_ERR_INVALID_ARG;
+    return guarded(c, [&] {
+        MS_REQUIRE(p && a, MS_ERR_INVALID_ARG, "params or atoms is NULL");
+        MS_REQUIRE(p->simulation_type == MS_SIM_HRTEM, MS_ERR_INVALID_ARG,
+                   "ms_simulate_tem_defocus_series runs HRTEM");
+        msb::DefocusSeries ser;
+        ser.n = n_defocus;
+        ser.df = defocus;
+        msb::sim_tem_like(c, *p, *a, out, false, &ser);
     });
 }
 

@@ -16,7 +16,6 @@ struct ms_ctx {
     std::string err;
     double last_ms = 0.0;
     int64_t last_launches = 0;
-    bool constants_ready = false;
     std::string prop_key;                        // parameters of the cached propagator table
     void* exptab = nullptr;                      // exp(2 pi i k / 1024), k < 1024
 
@@ -71,7 +70,13 @@ struct ms_ctx {
 
 namespace msb {
 void ctx_activate(ms_ctx* c);
-void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed);
+// A defocus series of HRTEM images: n offsets (Angstrom) added to the objective lens's C10.
+struct DefocusSeries {
+    int n = 0;
+    const double* df = nullptr;
+};
+void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed,
+                  const DefocusSeries* series = nullptr);
 void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out);
 void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out);
 void sim_potential(ms_ctx* c, const ms_params& p, const ms_atoms& a, int conf, float* V, int64_t cap, int on_dev,

@@ -298,6 +298,10 @@ Setup make_setup(ms_ctx* c, const ms_params& p)
     s.gd.alpha_f = (float)s.gc.alpha;
     s.gd.bwl = p.bwl ? 1 : 0;
     s.gd.inv_n = 1.0f / (float)s.N;
+    s.gd.lx = p.lx;
+    s.gd.ly = p.ly;
+    s.gd.g0x = s.gc.g0x;
+    s.gd.g0y = s.gc.g0y;
     s.tw_x = twiddles(c, p.nx);
     s.tw_y = twiddles(c, p.ny);
     // separable propagator phase exp(i w (g - g0)^2) per axis, formed in FP64 (device_kernels.cuh:215-234)
@@ -739,25 +743,29 @@ size_t fine_bytes_per_conf(const ms_params& p, const ms_atoms& a)
 
 }  // namespace
 
-void ctx_activate(ms_ctx* c)
-{
-    CK(cudaSetDevice(c->device));
-    if (!c->constants_ready) {
-        upload_constants(c->stream);
-        c->constants_ready = true;
-    }
-}
+void ctx_activate(ms_ctx* c) { CK(cudaSetDevice(c->device)); }
 
 // ---------------------------------------------------------------------------
 // HRTEM / ED (ED_HRTEM, single_simulator.cuh:11-126) and CBED (CBED_CBEI, :128-206)
 // ---------------------------------------------------------------------------
-void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed)
+void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed,
+                  const DefocusSeries* series)
 {
     validate_params(p);
     validate_atoms(p, &a);
     MS_REQUIRE(out != nullptr, MS_ERR_INVALID_ARG, "output is NULL");
     const bool kspace = force_cbed || p.simulation_type != MS_SIM_HRTEM;
     const bool full = p.data_record == MS_RECORD_WAVE;
+    const int nser = series ? series->n : 0;
+    if (series) {
+        MS_REQUIRE(!kspace, MS_ERR_INVALID_ARG, "a defocus series needs simulation_type HRTEM");
+        MS_REQUIRE(nser >= 1 && series->df != nullptr, MS_ERR_INVALID_ARG, "need at least one defocus value");
+        MS_REQUIRE(p.illumination_model == 0 || p.illumination_model == MS_ILLUM_COHERENT, MS_ERR_UNSUPPORTED,
+                   "a defocus series images with the coherent CTF (apply_CTF_kernel_batch)");
+        for (int i = 0; i < nser; i++)
+            MS_REQUIRE(std::isfinite(series->df[i]), MS_ERR_INVALID_ARG, "defocus values must be finite");
+    }
+    const int nimg = std::max(1, nser);
     MS_REQUIRE(full ? (out->image_real && out->image_imag) : (out->image_intensity != nullptr), MS_ERR_INVALID_ARG,
                "output buffers for the requested data_record are NULL");
     ctx_activate(c);
@@ -777,8 +785,8 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
                       fine_bytes_per_conf(p, a);
     int gsize = (int)std::max<size_t>(1, std::min<size_t>(cs.confs.size(), free_budget(c) / per_conf));
 
-    double* acc = (double*)c->buf("acc0", sizeof(double) * N);
-    double* acc_im = full ? (double*)c->buf("acc1", sizeof(double) * N) : nullptr;
+    double* acc = (double*)c->buf("acc0", sizeof(double) * N * nimg);
+    double* acc_im = full ? (double*)c->buf("acc1", sizeof(double) * N * nimg) : nullptr;
     bool first = true;
     int ns_first = 0;
     for (size_t g0 = 0; g0 < cs.confs.size(); g0 += gsize) {
@@ -815,11 +823,14 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
             run_col(c, p.ny, COL_PROBE_INV, pa, nw, p.nx, st);
         }
         const int S_max = *std::max_element(g.ns.begin(), g.ns.end());
+        const bool plane = iw == MS_IW_PLANE || iw == MS_IW_PLANE_TILTED;
         for (int sl = 0; sl < S_max; sl++) {
             pc.wait(c, sl);
             pa.slice = sl;
             pa.tw = s.tw_x;
-            run_row(c, p.nx, (sl == 0 && iw == MS_IW_PLANE) ? ROW_T_FWD : ROW_INV_T_FWD, pa, nw, p.ny, st);
+            PassArgs pr = pa;
+            if (sl == 0 && iw == MS_IW_PLANE_TILTED) pr.flags |= PF_TILT_INCIDENT;
+            run_row(c, p.nx, (sl == 0 && plane) ? ROW_T_FWD : ROW_INV_T_FWD, pr, nw, p.ny, st);
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_STEP, pa, nw, p.nx, st);
         }
@@ -865,6 +876,56 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
                         firstq = false;
                     }
             if (!full) launch_acc_real(img, nw, N, acc, first, st);
+        } else if (!kspace && nser > 0) {
+            // defocus series (apply_CTF_kernel_batch, device_kernels.cuh:469-503): the exit waves of the
+            // group are copied once per defocus value into one batch whose wave descriptors carry
+            // chi's defocus term -pi (C10 + df_i) lambda; one CTF column pass and one |.|^2 row pass
+            // cover the chunk, then each defocus value's images are summed over configurations
+            const int per = std::max(1, (int)std::min<int64_t>(nser, (int64_t)(free_budget(c) / 4 / ((size_t)N * 8 * nw))));
+            float2* q = (float2*)c->buf("ser_q", sizeof(float2) * N * nw * per);
+            float2* aux = full ? (float2*)c->buf("ser_aux", sizeof(float2) * N * nw * per) : nullptr;
+            float* img = full ? nullptr : (float*)c->buf("ser_img", sizeof(float) * N * nw * per);
+            WaveInfo* dwq = (WaveInfo*)c->buf("ser_waves", sizeof(WaveInfo) * nw * per);
+            std::vector<WaveInfo> wq((size_t)nw * per);
+            for (int d0 = 0; d0 < nser; d0 += per) {
+                const int nd = std::min(per, nser - d0);
+                for (int i = 0; i < nd; i++) {
+                    const double cc = gate_coef(-kPi * (p.obj_lens.c10 + series->df[d0 + i]) * s.ph.lambda);
+                    for (int w = 0; w < nw; w++) {
+                        wq[(size_t)i * nw + w] = wv[w];
+                        wq[(size_t)i * nw + w].cc10 = cc;
+                    }
+                    CK(cudaMemcpyAsync(q + (size_t)i * nw * N, psi, sizeof(float2) * N * nw, cudaMemcpyDeviceToDevice,
+                                       st));
+                }
+                CK(cudaMemcpyAsync(dwq, wq.data(), sizeof(WaveInfo) * nw * nd, cudaMemcpyHostToDevice, st));
+                PassArgs pq = pa;
+                pq.psi = q;
+                pq.waves = dwq;
+                pq.lens = obj;
+                pq.flags = PF_WAVE_DEFOCUS;
+                pq.tw = s.tw_y;
+                run_col(c, p.ny, COL_CTF_INV, pq, nw * nd, p.nx, st);
+                pq.flags = 0;
+                pq.tw = s.tw_x;
+                if (full) {
+                    pq.aux = aux;
+                    run_row(c, p.nx, ROW_INV_STORE, pq, nw * nd, p.ny, st);
+                } else {
+                    pq.out_real = img;
+                    run_row(c, p.nx, ROW_INV_ABS2, pq, nw * nd, p.ny, st);
+                }
+                for (int i = 0; i < nd; i++) {
+                    double* ai = acc + (size_t)(d0 + i) * N;
+                    if (full)
+                        launch_acc_cplx(aux + (size_t)i * nw * N, nw, dwq + (size_t)i * nw, N, ai,
+                                        acc_im + (size_t)(d0 + i) * N, first, st);
+                    else
+                        launch_acc_real(img + (size_t)i * nw * N, nw, N, ai, first, st);
+                }
+                // the host wave table is rewritten for the next chunk
+                CK(cudaStreamSynchronize(st));
+            }
         } else if (!kspace) {
             // OL_modulation -> CTF_TEM (wave_function.cuh:96-110, lens_modulation.cuh:78-89), or
             // PCTF_TEM (:91-110) with the partially coherent envelope
@@ -891,15 +952,16 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         first = false;
         CK(cudaStreamSynchronize(st));  // host wave table reused by the next group
     }
-    float* o0 = (float*)c->buf("out0", sizeof(float) * N);
-    launch_emit(acc, p.nx, p.ny, kspace ? 1 : 0, o0, st);
+    float* o0 = (float*)c->buf("out0", sizeof(float) * N * nimg);
+    for (int i = 0; i < nimg; i++) launch_emit(acc + (size_t)i * N, p.nx, p.ny, kspace ? 1 : 0, o0 + (size_t)i * N, st);
     if (full) {
-        copy_out(c, out->image_real, o0, N, out->on_device);
-        float* o1 = (float*)c->buf("out1", sizeof(float) * N);
-        launch_emit(acc_im, p.nx, p.ny, kspace ? 1 : 0, o1, st);
-        copy_out(c, out->image_imag, o1, N, out->on_device);
+        copy_out(c, out->image_real, o0, N * nimg, out->on_device);
+        float* o1 = (float*)c->buf("out1", sizeof(float) * N * nimg);
+        for (int i = 0; i < nimg; i++)
+            launch_emit(acc_im + (size_t)i * N, p.nx, p.ny, kspace ? 1 : 0, o1 + (size_t)i * N, st);
+        copy_out(c, out->image_imag, o1, N * nimg, out->on_device);
     } else {
-        copy_out(c, out->image_intensity, o0, N, out->on_device);
+        copy_out(c, out->image_intensity, o0, N * nimg, out->on_device);
     }
     tm.stop();
     out->row = p.ny;
@@ -1042,8 +1104,137 @@ void run_graphed(ms_ctx* c, const std::string& key, F&& body)
 }
 }  // namespace
 
+// General scan (run_STEM_general_simu, scan_simulator.cuh:115-183): for every phonon configuration
+// and probe position, the grid box is a window of lx x ly centred on the probe; the displaced atoms
+// inside it +- 2 A are cropped and shifted into the window (remove_atoms_outside_xy_range,
+// shift_atoms, :146-157), and the window is simulated with the probe at its centre.  A window
+// without atoms records the unscattered probe's detector intensity (the blank intensity, :159-166):
+// N^2 times the aperture pixels inside the detector.  The reference assigns each configuration's
+// weighted intensity over the previous one; here the configurations are summed with their weights.
+// Coordinates are cropped and shifted in float, as the reference's T = float code does.
+void sim_stem_general(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
+{
+    validate_params(p);
+    validate_atoms(p, &a);
+    MS_REQUIRE(p.simulation_type == MS_SIM_STEM, MS_ERR_INVALID_ARG, "simulation_type must be STEM");
+    MS_REQUIRE(out != nullptr && out->stem_intensity != nullptr, MS_ERR_INVALID_ARG, "stem_intensity is NULL");
+    ctx_activate(c);
+    cudaStream_t st = c->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } ev{e0, e1};
+    CK(cudaEventRecord(e0, st));
+    const int64_t l0 = kernel_launches();
+    const int npos = p.scan_nx * p.scan_ny, ndet = p.n_det;
+    const int64_t N = (int64_t)p.nx * p.ny;
+    const Physics ph = physics_of(p.E0, p.theta);
+    // blank intensity per detector: N^2 per aperture pixel inside the detector's annulus
+    std::vector<double> blank((size_t)ndet, 0.0);
+    {
+        const GridConst gc = grid_of(p, ph);
+        const LensCoef L = lens_coef(p.cond_lens, ph.lambda, 0.0);
+        for (int d = 0; d < ndet; d++) {
+            const float gi = g2_threshold(p.det_inner[d], ph.lambda), go = g2_threshold(p.det_outer[d], ph.lambda);
+            double cnt = 0.0;
+            for (int iy = 0; iy < p.ny; iy++)
+                for (int ix = 0; ix < p.nx; ix++) {
+                    const float g2 = det_g2(ix, iy, p.nx, p.ny, gc.dgx_f, gc.dgy_f);
+                    if (L.g2min <= g2 && g2 < L.g2max && gi <= g2 && g2 <= go) cnt += 1.0;
+                }
+            blank[d] = cnt * (double)N * (double)N;
+        }
+    }
+    ConfSet cs = conf_set(p);
+    std::vector<double> img((size_t)ndet * npos, 0.0);
+    std::vector<float> xd(a.n), yd(a.n), zd(a.n);
+    std::vector<int> cz;
+    std::vector<float> cx, cy, czz, csig, cocc;
+    ms_params q = p;
+    q.phonon_model = MS_PHONON_STILL;   // the cropped atoms are already displaced
+    q.pn_nconf = 1;
+    q.exec_mode = MS_EXEC_BATCHED;
+    q.scan_nx = q.scan_ny = 1;
+    q.scan_x0 = 0.5 * p.lx;
+    q.scan_y0 = 0.5 * p.ly;
+    q.scan_dx = q.scan_dy = 0.0;
+    q.probe_batch = 1;
+    std::vector<float> Iw((size_t)ndet);
+    for (int conf : cs.confs) {
+        host_displace(p, a, conf, xd.data(), yd.data(), zd.data());
+        for (int ip = 0; ip < npos; ip++) {
+            const int ix = ip % p.scan_nx, iy = ip / p.scan_nx;
+            const double px = p.scan_x0 + ix * p.scan_dx, py = p.scan_y0 + iy * p.scan_dy;
+            const float xs = (float)(px - 0.5 * p.lx), ys = (float)(py - 0.5 * p.ly);
+            const float xlo = xs - 2.0f, xhi = (xs + (float)p.lx) + 2.0f;
+            const float ylo = ys - 2.0f, yhi = (ys + (float)p.ly) + 2.0f;
+            cz.clear(); cx.clear(); cy.clear(); czz.clear(); csig.clear(); cocc.clear();
+            for (int64_t k = 0; k < a.n; k++) {
+                if (xd[k] < xlo || xd[k] > xhi || yd[k] < ylo || yd[k] > yhi) continue;
+                cz.push_back(a.Z[k]);
+                cx.push_back(xd[k] - xs);
+                cy.push_back(yd[k] - ys);
+                czz.push_back(zd[k]);
+                csig.push_back(a.sigma ? a.sigma[k] : 0.0f);
+                cocc.push_back(a.occ ? a.occ[k] : 1.0f);
+            }
+            if (cz.empty()) {
+                for (int d = 0; d < ndet; d++) img[(size_t)d * npos + ip] += cs.weight * blank[d];
+                continue;
+            }
+            ms_atoms w;
+            w.n = (int64_t)cz.size();
+            w.Z = cz.data();
+            w.x = cx.data();
+            w.y = cy.data();
+            w.z = czz.data();
+            w.sigma = csig.data();
+            w.occ = cocc.data();
+            ms_output o;
+            std::memset(&o, 0, sizeof(o));
+            o.stem_intensity = Iw.data();
+            sim_stem(c, q, w, &o);
+            for (int d = 0; d < ndet; d++) img[(size_t)d * npos + ip] += cs.weight * (double)Iw[d];
+        }
+    }
+    std::vector<float> res(img.size());
+    for (size_t k = 0; k < img.size(); k++) res[k] = (float)img[k];
+    CK(cudaMemcpyAsync(out->stem_intensity, res.data(), sizeof(float) * res.size(),
+                       out->on_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost, st));
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    c->last_ms = ms;
+    c->last_launches = kernel_launches() - l0;
+    c->last_batch = 1;
+    out->row = p.scan_ny;
+    out->col = p.scan_nx;
+    out->interval_x = p.scan_dx;
+    out->interval_y = p.scan_dy;
+    out->n_slices = 0;
+    double tot = 0.0;
+    {
+        const GridConst gc = grid_of(p, ph);
+        const LensCoef L = lens_coef(p.cond_lens, ph.lambda, 0.0);
+        for (int iy = 0; iy < p.ny; iy++)
+            for (int ix = 0; ix < p.nx; ix++) {
+                const float g2 = det_g2(ix, iy, p.nx, p.ny, gc.dgx_f, gc.dgy_f);
+                if (L.g2min <= g2 && g2 < L.g2max) tot += 1.0;
+            }
+    }
+    out->total_intensity = tot * (double)N * (double)N;
+}
+
 void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
 {
+    if (p.exec_mode == MS_EXEC_GENERAL) {
+        sim_stem_general(c, p, a, out);
+        return;
+    }
     validate_params(p);
     validate_atoms(p, &a);
     MS_REQUIRE(p.simulation_type == MS_SIM_STEM, MS_ERR_INVALID_ARG, "simulation_type must be STEM");
@@ -1236,7 +1427,8 @@ void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* 
             pa.slice = sl;
             pa.flags = PF_VACUUM_BEYOND;
             pa.tw = s.tw_x;
-            run_row(c, p.nx, (sl == 0 && iw == MS_IW_PLANE) ? ROW_T_FWD : ROW_INV_T_FWD, pa, 1, p.ny, st);
+            if (sl == 0 && iw == MS_IW_PLANE_TILTED) pa.flags |= PF_TILT_INCIDENT;
+            run_row(c, p.nx, (sl == 0 && iw != MS_IW_CONVERGENT) ? ROW_T_FWD : ROW_INV_T_FWD, pa, 1, p.ny, st);
             pa.flags = PF_VACUUM_BEYOND | PF_PROP_ALWAYS | PF_FILTER_AUX;
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_STEP, pa, 1, p.nx, st);
@@ -1656,6 +1848,10 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             s0.gd.alpha_f = (float)gc.alpha;
             s0.gd.bwl = p.bwl ? 1 : 0;
             s0.gd.inv_n = 1.0f / (float)N;
+            s0.gd.lx = p.lx;
+            s0.gd.ly = p.ly;
+            s0.gd.g0x = gc.g0x;
+            s0.gd.g0y = gc.g0y;
             I.gd = s0.gd;
             I.cond = lens_dev(lens_coef(p.cond_lens, ph.lambda, 0.0));
             AtomsDev A = upload_atoms(c, p, as[i]);

@@ -21,13 +21,85 @@
 
 #include "fft_layout.hpp"
 
+// Twiddle precision: 1 carries the register-DFT constants (MS_SPLIT_REG) and the inter-level
+// twiddles (MS_SPLIT_LEVEL) as hi + lo float pairs, 0 as one float.
+#ifndef MS_SPLIT_REG
+#define MS_SPLIT_REG 1
+#endif
+#ifndef MS_SPLIT_LEVEL
+#define MS_SPLIT_LEVEL 1
+#endif
+
 namespace msb {
 
-// W_64^m = exp(-2 pi i m / 64) as an unevaluated sum hi + lo of two floats (hi rounded from
-// FP64, lo the rounded remainder), uploaded by upload_constants.  Defined here: only
-// kernels.cu includes this header.
-__constant__ float2 c_tw64[64];
-__constant__ float2 c_tw64_lo[64];
+// W_64^m = exp(-2 pi i m / 64) as an unevaluated sum hi + lo of two floats: hi is the double
+// value rounded to float, lo the rounded remainder.  The values are computed at compile time
+// (tw64::cos_m / sin_m: the octant by an exact rotation, the remainder angle below pi/4 by its
+// Taylor series in double), so every translation unit's copy of the table is initialised in its
+// module image and nothing is uploaded at run time.
+namespace tw64 {
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kRsqrt2 = 0.70710678118654752440084436210484903928;
+// sin a and cos a for 0 <= a <= pi/4 (terms to a^41: truncation far below double rounding)
+constexpr double sin_series(double a)
+{
+    double t = a, s = a;
+    for (int k = 1; k <= 20; k++) {
+        t *= -a * a / ((2.0 * k) * (2.0 * k + 1.0));
+        s += t;
+    }
+    return s;
+}
+constexpr double cos_series(double a)
+{
+    double t = 1.0, s = 1.0;
+    for (int k = 1; k <= 20; k++) {
+        t *= -a * a / ((2.0 * k - 1.0) * (2.0 * k));
+        s += t;
+    }
+    return s;
+}
+// cos and sin of 2 pi m / 64 = q pi/4 + r pi/32 with q = m / 8, r = m % 8
+constexpr double cq_of(int q) { return q == 0 ? 1.0 : q == 1 ? kRsqrt2 : q == 2 ? 0.0 : q == 3 ? -kRsqrt2 : q == 4 ? -1.0 : q == 5 ? -kRsqrt2 : q == 6 ? 0.0 : kRsqrt2; }
+constexpr double sq_of(int q) { return q == 0 ? 0.0 : q == 1 ? kRsqrt2 : q == 2 ? 1.0 : q == 3 ? kRsqrt2 : q == 4 ? 0.0 : q == 5 ? -kRsqrt2 : q == 6 ? -1.0 : -kRsqrt2; }
+constexpr double cos_m(int m)
+{
+    const double a = kPi * (m % 8) / 32.0;
+    return cq_of(m / 8) * cos_series(a) - sq_of(m / 8) * sin_series(a);
+}
+constexpr double sin_m(int m)
+{
+    const double a = kPi * (m % 8) / 32.0;
+    return sq_of(m / 8) * cos_series(a) + cq_of(m / 8) * sin_series(a);
+}
+}  // namespace tw64
+
+// entry m of the forward twiddle exp(-i 2 pi m / 64) = (cos, -sin)
+#define MS_TW_HI(m) float2{(float)tw64::cos_m(m), (float)(-tw64::sin_m(m))}
+#define MS_TW_LO(m) float2{(float)(tw64::cos_m(m) - (double)(float)tw64::cos_m(m)), \
+                           (float)(-tw64::sin_m(m) - (double)(float)(-tw64::sin_m(m)))}
+static __constant__ float2 c_tw64[64] = {
+    MS_TW_HI(0), MS_TW_HI(1), MS_TW_HI(2), MS_TW_HI(3), MS_TW_HI(4), MS_TW_HI(5), MS_TW_HI(6), MS_TW_HI(7),
+    MS_TW_HI(8), MS_TW_HI(9), MS_TW_HI(10), MS_TW_HI(11), MS_TW_HI(12), MS_TW_HI(13), MS_TW_HI(14), MS_TW_HI(15),
+    MS_TW_HI(16), MS_TW_HI(17), MS_TW_HI(18), MS_TW_HI(19), MS_TW_HI(20), MS_TW_HI(21), MS_TW_HI(22), MS_TW_HI(23),
+    MS_TW_HI(24), MS_TW_HI(25), MS_TW_HI(26), MS_TW_HI(27), MS_TW_HI(28), MS_TW_HI(29), MS_TW_HI(30), MS_TW_HI(31),
+    MS_TW_HI(32), MS_TW_HI(33), MS_TW_HI(34), MS_TW_HI(35), MS_TW_HI(36), MS_TW_HI(37), MS_TW_HI(38), MS_TW_HI(39),
+    MS_TW_HI(40), MS_TW_HI(41), MS_TW_HI(42), MS_TW_HI(43), MS_TW_HI(44), MS_TW_HI(45), MS_TW_HI(46), MS_TW_HI(47),
+    MS_TW_HI(48), MS_TW_HI(49), MS_TW_HI(50), MS_TW_HI(51), MS_TW_HI(52), MS_TW_HI(53), MS_TW_HI(54), MS_TW_HI(55),
+    MS_TW_HI(56), MS_TW_HI(57), MS_TW_HI(58), MS_TW_HI(59), MS_TW_HI(60), MS_TW_HI(61), MS_TW_HI(62), MS_TW_HI(63)
+};
+static __constant__ float2 c_tw64_lo[64] = {
+    MS_TW_LO(0), MS_TW_LO(1), MS_TW_LO(2), MS_TW_LO(3), MS_TW_LO(4), MS_TW_LO(5), MS_TW_LO(6), MS_TW_LO(7),
+    MS_TW_LO(8), MS_TW_LO(9), MS_TW_LO(10), MS_TW_LO(11), MS_TW_LO(12), MS_TW_LO(13), MS_TW_LO(14), MS_TW_LO(15),
+    MS_TW_LO(16), MS_TW_LO(17), MS_TW_LO(18), MS_TW_LO(19), MS_TW_LO(20), MS_TW_LO(21), MS_TW_LO(22), MS_TW_LO(23),
+    MS_TW_LO(24), MS_TW_LO(25), MS_TW_LO(26), MS_TW_LO(27), MS_TW_LO(28), MS_TW_LO(29), MS_TW_LO(30), MS_TW_LO(31),
+    MS_TW_LO(32), MS_TW_LO(33), MS_TW_LO(34), MS_TW_LO(35), MS_TW_LO(36), MS_TW_LO(37), MS_TW_LO(38), MS_TW_LO(39),
+    MS_TW_LO(40), MS_TW_LO(41), MS_TW_LO(42), MS_TW_LO(43), MS_TW_LO(44), MS_TW_LO(45), MS_TW_LO(46), MS_TW_LO(47),
+    MS_TW_LO(48), MS_TW_LO(49), MS_TW_LO(50), MS_TW_LO(51), MS_TW_LO(52), MS_TW_LO(53), MS_TW_LO(54), MS_TW_LO(55),
+    MS_TW_LO(56), MS_TW_LO(57), MS_TW_LO(58), MS_TW_LO(59), MS_TW_LO(60), MS_TW_LO(61), MS_TW_LO(62), MS_TW_LO(63)
+};
+#undef MS_TW_HI
+#undef MS_TW_LO
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -68,7 +140,7 @@ __device__ __forceinline__ float2 tw_apply(float2 d, int m)
     if (m == 8 || m == 24) {
         // W_64^8 = (1 - i)/sqrt2 and W_64^24 = (-1 - i)/sqrt2 (their conjugates for DIR > 0): a sum
         // and a difference of the two parts, each scaled by 1/sqrt2 carried as hi + lo
-        const float hs = c_tw64[8].x, ls = c_tw64_lo[8].x;
+        const float hs = c_tw64[8].x, ls = MS_SPLIT_REG ? c_tw64_lo[8].x : 0.0f;
         float re, im;
         if (DIR < 0) {
             re = (m == 8) ? d.x + d.y : d.y - d.x;
@@ -79,6 +151,7 @@ __device__ __forceinline__ float2 tw_apply(float2 d, int m)
         }
         return make_float2(fmaf(re, hs, re * ls), fmaf(im, hs, im * ls));
     }
+    if (!MS_SPLIT_REG) return DIR < 0 ? cmul(d, c_tw64[m]) : cmulc(d, c_tw64[m]);
     return DIR < 0 ? cmul_split(d, c_tw64[m], c_tw64_lo[m]) : cmulc_split(d, c_tw64[m], c_tw64_lo[m]);
 }
 
@@ -128,7 +201,12 @@ __device__ __forceinline__ void team_fft(float2 (&v)[N / G], int g, const float2
     dft_reg<E, DIR>(v);
 #pragma unroll
     for (int k1 = 1; k1 < E; k1++) {
-        const float2 wh = tw[k1 * G + g], wl = tw[N + k1 * G + g];
+        const float2 wh = tw[k1 * G + g];
+        if (!MS_SPLIT_LEVEL) {
+            v[brev<E>(k1)] = DIR < 0 ? cmul(v[brev<E>(k1)], wh) : cmulc(v[brev<E>(k1)], wh);
+            continue;
+        }
+        const float2 wl = tw[N + k1 * G + g];
         v[brev<E>(k1)] = DIR < 0 ? cmul_split(v[brev<E>(k1)], wh, wl) : cmulc_split(v[brev<E>(k1)], wh, wl);
     }
     sync();

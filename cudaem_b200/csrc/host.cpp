@@ -364,6 +364,10 @@ void validate_params(const ms_params& p)
     MS_REQUIRE(p.dz > 0 && std::isfinite(p.dz), MS_ERR_INVALID_ARG, "dz must be positive");
     MS_REQUIRE(p.E0 > 0 && p.E0 < 10000, MS_ERR_INVALID_ARG, "E0 must be in (0, 10000) kV");
     MS_REQUIRE(std::fabs(p.theta) < 1.0, MS_ERR_INVALID_ARG, "beam tilt theta out of range");
+    MS_REQUIRE(p.iw_type <= 0 || (p.iw_type >= MS_IW_PLANE && p.iw_type <= MS_IW_PLANE_TILTED), MS_ERR_INVALID_ARG,
+               "iw_type must be plane, convergent or tilted plane (or <= 0 for the mode's default)");
+    MS_REQUIRE(p.exec_mode >= MS_EXEC_BATCHED && p.exec_mode <= MS_EXEC_GENERAL, MS_ERR_INVALID_ARG,
+               "exec_mode must be batched, plain or general");
     MS_REQUIRE(p.enable_fine_slicing == 0 || p.enable_fine_slicing == 1, MS_ERR_INVALID_ARG,
                "enable_fine_slicing must be 0 or 1");
     MS_REQUIRE(p.illumination_model == 0 || (p.illumination_model >= MS_ILLUM_COHERENT && p.illumination_model <= MS_ILLUM_TCC),
@@ -399,7 +403,6 @@ void validate_params(const ms_params& p)
         MS_REQUIRE((int64_t)p.scan_nx * p.scan_ny <= (1LL << 26), MS_ERR_INVALID_ARG, "scan too large");
         MS_REQUIRE(p.n_det >= 1, MS_ERR_INVALID_ARG, "STEM needs at least one detector");
     }
-    MS_REQUIRE(p.exec_mode == MS_EXEC_BATCHED || p.exec_mode == MS_EXEC_PLAIN, MS_ERR_INVALID_ARG, "exec_mode");
     MS_REQUIRE(p.probe_batch >= 0 && p.probe_batch <= 4096, MS_ERR_INVALID_ARG, "probe_batch out of range");
 }
 

@@ -26,6 +26,8 @@ struct GridDev {
     float gl2_f, alpha_f;
     int bwl;
     float inv_n;
+    double lx, ly;     // box, Angstrom
+    double g0x, g0y;   // beam tilt as a spatial frequency (gx_0, gy_0: multislice_params_dev.cuh:201-208)
 };
 
 struct LensDev {
@@ -67,7 +69,9 @@ enum PassFlags {
     PF_FILTER_AUX = 4,     // COL_STEP also writes the annulus-filtered spectrum to aux
     PF_PROP_ALWAYS = 8,    // COL_STEP propagates even after the wave's last slice
     PF_STORE_X = 16,       // ROW_INV_T_FWD also writes the transmitted real-space wave to xs
-    PF_CONJ_PROP = 32      // COL_STEP multiplies by conj(P) (the adjoint step)
+    PF_CONJ_PROP = 32,     // COL_STEP multiplies by conj(P) (the adjoint step)
+    PF_WAVE_DEFOCUS = 64,  // COL_CTF_INV takes each wave's own defocus term (WaveInfo.cc10) instead of the lens's
+    PF_TILT_INCIDENT = 128 // ROW_T_FWD / ROW_TT_FWD start from the tilted plane wave exp(2 pi i g0.(r - L/2))
 };
 
 struct PassArgs {
@@ -141,8 +145,13 @@ struct PotArgs {
 
 struct ElemCoefDev;
 
+// slice passes of one transform length (passes_<N>.cu)
+template <int N>
+void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st);
+template <int N>
+void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
+
 // launchers (kernels.cu); all asynchronous on `st`
-void upload_constants(cudaStream_t st);
 void launch_row(int N, int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st);
 void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
 size_t row_smem(int N);

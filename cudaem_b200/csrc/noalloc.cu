@@ -13,12 +13,19 @@
 //
 // The array is created when the library's module for this file is loaded on
 // a device and stays until the process exits (about 34 MiB per GPU).  Its
-// device address is looked up once per device, on the first call made with
-// that device current; that first call should therefore come before any
-// stream capture.  Every call shares the one array, so calls that overlap on
-// the GPU (different streams, or host threads) race on it and must be
-// serialised by the caller.  Nothing in the array needs to start at zero:
-// each call writes every value before reading it.
+// device address is looked up on the first call made with that device
+// current (and again whenever the device's CUDA context has changed, e.g.
+// after cudaDeviceReset); that first call should therefore come before any
+// stream capture.  Every call synchronises the stream after each probe batch,
+// so it returns only when its results are in the caller's output.  Every call
+// shares the one array, so calls that overlap on the GPU (different streams,
+// or host threads) race on it and must be serialised by the caller.  Nothing
+// in the array needs to start at zero: each call writes every value before
+// reading it.  The FFT and propagator tables of the last grid stay in the
+// array and are not uploaded again while the grid, beam and slice thickness
+// are unchanged.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -57,30 +64,71 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
 std::mutex g_mtx;
-void* g_addr[128] = {nullptr};
-bool g_const_ready[128] = {false};
 
-// Device address of the scratch array on the current device (looked up once per device).
-unsigned char* scratch_for_current_device(cudaStream_t st)
+// What the array holds on one device: the CUDA context it was set up in, its device address, and
+// the key of the FFT / propagator tables it currently holds.
+struct TableKey {
+    int nx, ny;
+    double dgx, dgy, g0x, g0y, prop_w;
+};
+struct DevState {
+    unsigned long long ctx_id = 0;
+    unsigned char* addr = nullptr;
+    bool have_tables = false;
+    TableKey key{};
+};
+DevState g_state[128];
+
+// Identifier of the calling thread's current CUDA context (cuCtxGetId through the runtime's
+// driver entry points; no link against the driver library).  0 when no context is current yet
+// or the driver does not provide the call, which makes every call set up again.
+unsigned long long current_context_id()
+{
+    static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (PFN_cuCtxGetCurrent_v4000)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (PFN_cuCtxGetId_v12000)f;
+        cudaGetLastError();
+        looked_up = true;
+    }
+    if (!get_cur || !get_id) return 0;
+    CUcontext cx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&cx) != CUDA_SUCCESS || !cx || get_id(cx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Set-up on the current device: the device address of the scratch array (cudaGetSymbolAddress;
+// the array's name is only a host-side stand-in).  Done on the first call with this device current
+// and again whenever the current context differs from the one the set-up was made in (a reset
+// device reloads the modules, and the array may move; the tables it held are gone).  The caller
+// holds g_mtx.
+DevState& setup_current_device()
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) throw MsError(MS_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     MS_REQUIRE(dev >= 0 && dev < 128, MS_ERR_NO_DEVICE, "device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_mtx);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            throw MsError(MS_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array: ") +
-                                           cudaGetErrorString(e));
-        g_addr[dev] = p;
-    }
-    if (!g_const_ready[dev]) {
-        upload_constants(st);
-        g_const_ready[dev] = true;
-    }
-    return (unsigned char*)g_addr[dev];
+    DevState& s = g_state[dev];
+    unsigned long long id = current_context_id();
+    if (id != 0 && id == s.ctx_id && s.addr) return s;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        throw MsError(MS_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array: ") + cudaGetErrorString(e));
+    s.addr = (unsigned char*)p;
+    s.ctx_id = current_context_id();   // the look-up above made the device's context current
+    s.have_tables = false;
+    return s;
 }
 
 int team_size_of(int N)
@@ -126,9 +174,60 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
     MS_REQUIRE(S >= 1 && np >= 1, MS_ERR_INVALID_ARG, "need at least one slice and one probe");
     MS_REQUIRE(p.n_det >= 1 && p.n_det <= MS_MAX_DET, MS_ERR_INVALID_ARG, "need 1..8 detectors");
     const int64_t N = (int64_t)p.nx * p.ny;
+    // validate_params already caps each axis at 2048 points, which is exactly this limit; the check
+    // keeps the array's size and the accepted grids tied together if either changes
     MS_REQUIRE((size_t)N * sizeof(float2) <= kWaveBytes, MS_ERR_UNSUPPORTED,
                "grid too large for the fixed scratch array: nx*ny*8 bytes must not exceed 32 MiB");
-    unsigned char* base = scratch_for_current_device(st);
+    Physics ph = physics_of(p.E0, p.theta);
+    GridConst gc = grid_of(p, ph);
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mtx);
+        DevState& ds = setup_current_device();
+        base = ds.addr;
+        float2* tw_x = (float2*)(base + kOffTables);
+        float2* tw_y = tw_x + 2 * kMaxN;
+        float2* prop_x = tw_y + 2 * kMaxN;
+        float2* prop_y = prop_x + kMaxN;
+        float2* exptab = prop_y + kMaxN;
+        const TableKey key{p.nx, p.ny, gc.dgx, gc.dgy, gc.g0x, gc.g0y, gc.prop_w};
+        if (!ds.have_tables) {
+            // the exp(i phi) table depends on nothing; it is uploaded once per set-up
+            std::vector<float2> et(kExpN);
+            for (int k = 0; k < kExpN; k++) {
+                double e = 2.0 * 3.14159265358979323846264338327950288 * k / (double)kExpN;
+                et[k] = make_float2((float)std::cos(e), (float)std::sin(e));
+            }
+            ck(cudaMemcpyAsync(exptab, et.data(), sizeof(float2) * kExpN, cudaMemcpyHostToDevice, st), "table upload");
+        }
+        if (!ds.have_tables || std::memcmp(&key, &ds.key, sizeof(key)) != 0) {
+            // only the entries this grid uses: 2 nx + 2 ny twiddles, nx + ny propagator factors
+            ds.have_tables = false;
+            std::vector<float2> tab(3 * (size_t)(p.nx + p.ny));
+            float2* tx = tab.data();
+            float2* ty = tx + 2 * p.nx;
+            float2* px = ty + 2 * p.ny;
+            float2* py = px + p.nx;
+            twiddle_table(p.nx, tx);
+            twiddle_table(p.ny, ty);
+            for (int i = 0; i < p.nx; i++) {
+                double g = (double)((i < p.nx / 2) ? i : i - p.nx) * gc.dgx - gc.g0x;
+                double th = gc.prop_w * g * g;
+                px[i] = make_float2((float)std::cos(th), (float)std::sin(th));
+            }
+            for (int i = 0; i < p.ny; i++) {
+                double g = (double)((i < p.ny / 2) ? i : i - p.ny) * gc.dgy - gc.g0y;
+                double th = gc.prop_w * g * g;
+                py[i] = make_float2((float)std::cos(th), (float)std::sin(th));
+            }
+            ck(cudaMemcpyAsync(tw_x, tx, sizeof(float2) * 2 * p.nx, cudaMemcpyHostToDevice, st), "table upload");
+            ck(cudaMemcpyAsync(tw_y, ty, sizeof(float2) * 2 * p.ny, cudaMemcpyHostToDevice, st), "table upload");
+            ck(cudaMemcpyAsync(prop_x, px, sizeof(float2) * p.nx, cudaMemcpyHostToDevice, st), "table upload");
+            ck(cudaMemcpyAsync(prop_y, py, sizeof(float2) * p.ny, cudaMemcpyHostToDevice, st), "table upload");
+            ds.key = key;
+            ds.have_tables = true;
+        }
+    }
     float2* tw_x = (float2*)(base + kOffTables);
     float2* tw_y = tw_x + 2 * kMaxN;
     float2* prop_x = tw_y + 2 * kMaxN;
@@ -139,27 +238,6 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
     double* Iw = (double*)(base + kOffIwave);
     double* partial = (double*)(base + kOffPartial);
     float2* psi = (float2*)(base + kOffWave);
-
-    Physics ph = physics_of(p.E0, p.theta);
-    GridConst gc = grid_of(p, ph);
-    std::vector<float2> tab(6 * (size_t)kMaxN + kExpN);
-    for (int k = 0; k < kExpN; k++) {
-        double e = 2.0 * 3.14159265358979323846264338327950288 * k / (double)kExpN;
-        tab[6 * (size_t)kMaxN + k] = make_float2((float)std::cos(e), (float)std::sin(e));
-    }
-    twiddle_table(p.nx, tab.data());
-    twiddle_table(p.ny, tab.data() + 2 * kMaxN);
-    for (int i = 0; i < p.nx; i++) {
-        double g = (double)((i < p.nx / 2) ? i : i - p.nx) * gc.dgx - gc.g0x;
-        double th = gc.prop_w * g * g;
-        tab[4 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
-    }
-    for (int i = 0; i < p.ny; i++) {
-        double g = (double)((i < p.ny / 2) ? i : i - p.ny) * gc.dgy - gc.g0y;
-        double th = gc.prop_w * g * g;
-        tab[5 * kMaxN + i] = make_float2((float)std::cos(th), (float)std::sin(th));
-    }
-    ck(cudaMemcpyAsync(tw_x, tab.data(), kTableBytes, cudaMemcpyHostToDevice, st), "table upload");
     const int ndet = p.n_det;
     float th_h[2 * MS_MAX_DET];
     for (int d = 0; d < ndet; d++) {
@@ -179,6 +257,10 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
     gd.alpha_f = (float)gc.alpha;
     gd.bwl = p.bwl ? 1 : 0;
     gd.inv_n = 1.0f / (float)N;
+    gd.lx = p.lx;
+    gd.ly = p.ly;
+    gd.g0x = gc.g0x;
+    gd.g0y = gc.g0y;
     LensCoef lc = lens_coef(p.cond_lens, ph.lambda, 0.0);
     LensDev lens;
     std::memset(&lens, 0, sizeof(lens));

@@ -1,0 +1,9 @@
+// Slice-pass kernels for transforms of 2048 points.
+#include "passes.cuh"
+
+namespace msb {
+
+template void row_dispatch<2048>(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st);
+template void col_dispatch<2048>(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
+
+}  // namespace msb

@@ -57,8 +57,10 @@ typedef enum ms_status {
 enum { MS_SIM_HRTEM = 1, MS_SIM_ED = 2, MS_SIM_CBED = 3, MS_SIM_STEM = 4 };
 /* ePhonon_Model (multislice_params_dev.cuh:25) */
 enum { MS_PHONON_STILL = 1, MS_PHONON_FROZEN = 3 };
-/* eIncident_Wave_Type (incident_wave.cuh:29-46) */
-enum { MS_IW_PLANE = 1, MS_IW_CONVERGENT = 2 };
+/* eIncident_Wave_Type (incident_wave.cuh:29-46); MS_IW_PLANE_TILTED is the plane wave times the
+ * beam-tilt factor exp(2 pi i g0.(r - L/2)) of Incident_Wave::apply_beam_tilt (incident_wave.cuh:72-78,
+ * exp_r_factor_2d, device_kernels.cuh:519-533) with g0 = sin(theta)(cos phi, sin phi)/lambda */
+enum { MS_IW_PLANE = 1, MS_IW_CONVERGENT = 2, MS_IW_PLANE_TILTED = 3 };
 /* ePotential_Type (basic_functions_dev.cuh:187-214); MS_POT_MOLIERE is this engine's built-in table */
 enum {
     MS_POT_DOYLE_0_4 = 1, MS_POT_PENG_0_4 = 2, MS_POT_PENG_0_12 = 3, MS_POT_KIRKLAND_0_12 = 4,
@@ -72,8 +74,13 @@ enum { MS_ILLUM_COHERENT = 1, MS_ILLUM_PARTIAL = 2, MS_ILLUM_TCC = 3 };
 enum { MS_TSI_TEMPORAL_SPATIAL = 1, MS_TSI_TEMPORAL = 2, MS_TSI_SPATIAL = 3, MS_TSI_COHERENT = 4 };
 /* data_record (multislice_params_dev.cuh:117): intensity or full complex wave */
 enum { MS_RECORD_INTENSITY = 0, MS_RECORD_WAVE = 1 };
-/* execution form of the STEM scan: batched probes (tile scan) or one probe per launch (general scan) */
-enum { MS_EXEC_BATCHED = 0, MS_EXEC_PLAIN = 1 };
+/* execution form of the STEM scan: batched probes on the whole specimen (tile scan,
+ * run_STEM_tile_simu, scan_simulator.cuh:11-113); one probe per launch on the whole specimen
+ * (the plain comparator); or the general scan (run_STEM_general_simu, scan_simulator.cuh:115-183):
+ * per probe position the grid box is a window of lx x ly centred on the probe, the atoms of the
+ * displaced specimen inside it +- 2 A are cropped and shifted into it, and a window without atoms
+ * records the unscattered probe's detector intensity */
+enum { MS_EXEC_BATCHED = 0, MS_EXEC_PLAIN = 1, MS_EXEC_GENERAL = 2 };
 /* eMatch_Border for slicing (slice_generator.hpp:130-168) */
 enum { MS_BORDER_MIN = 0, MS_BORDER_MAX = 1, MS_BORDER_MIDDLE = 2 };
 
@@ -230,6 +237,16 @@ ms_status ms_physics(double E0_kV, double* lambda, double* sigma, double* gamma)
 /* ---- simulator entry points ---------------------------------------------- */
 /* mulSimulator::executionTEM (simulator.cu:8-19): HRTEM image or ED pattern. */
 ms_status ms_simulate_tem(ms_ctx* ctx, const ms_params* p, const ms_atoms* atoms, ms_output* out);
+/* Defocus series of HRTEM images from one multislice run: the exit waves are imaged through the
+ * objective lens at C10 + defocus[i] for i < n_defocus, each image summed over the phonon
+ * configurations (apply_CTF_kernel_batch, device_kernels.cuh:469-503, which adds defocus[i] g^2 to
+ * the lens phase of a batch of copies of the exit wave; the reference defines it without a
+ * driver, so the batch is exposed here as its own entry point).  Coherent CTF only
+ * (illumination_model coherent).  out->image_intensity (data_record intensity) or
+ * out->image_real / out->image_imag (data_record wave) hold n_defocus*ny*nx floats, laid out
+ * [defocus][row][col]. */
+ms_status ms_simulate_tem_defocus_series(ms_ctx* ctx, const ms_params* p, const ms_atoms* atoms, int n_defocus,
+                                         const double* defocus, ms_output* out);
 /* mulSimulator::executionCBED (simulator.cu:20-30): CBED pattern. */
 ms_status ms_simulate_cbed(ms_ctx* ctx, const ms_params* p, const ms_atoms* atoms, ms_output* out);
 /* mulSimulator::executionSTEM (simulator.cu:31-49): annular-detector STEM image. */
@@ -278,9 +295,13 @@ ms_status ms_stem_forward_potential(ms_ctx* ctx, const ms_params* p, const float
  * of the current device.  All scratch -- waves, twiddles, propagator factors, detector
  * partial sums -- lives in one fixed array of about 34 MiB held by every GPU that loads the
  * library until exit; grids with nx*ny*8 bytes above 32 MiB (larger than 2048 x 2048) are
- * rejected with MS_ERR_UNSUPPORTED.  The first call on each device looks the array up and
- * should come before any stream capture.  All calls share the array, so calls that overlap
- * on the GPU race and must be serialised.  Errors are read with ms_last_error(NULL). */
+ * rejected with MS_ERR_UNSUPPORTED.  The first call on each device looks the array up (again
+ * after the device's CUDA context changes, e.g. after cudaDeviceReset); that first call should
+ * come before any stream capture.  The call uploads
+ * probe positions from host memory and synchronises the stream after every probe batch, so it
+ * blocks the host until its results are in I_out.  All calls share the array, so calls that
+ * overlap on the GPU race and must be serialised.  Errors are read with ms_last_error(NULL),
+ * which a successful call clears. */
 ms_status ms_stem_forward_potential_noalloc(void* cuda_stream, const ms_params* p, const float* V, int n_slices,
                                             double z_init, const double* probe_xy, int n_probe, float* I_out);
 /* Adjoint of ms_stem_forward_potential for the loss L = sum_{probe,det} (I - target)^2:

@@ -1240,11 +1240,100 @@ static void or_detect(const ms_params* p, const or_sim* s, const cplx* W, double
         }
 }
 
+/* run_STEM_general_simu (scan_simulator.cuh:115-183): per configuration and probe position, the
+   displaced atoms inside the probe-centred window (lx x ly) +- 2 A are cropped and shifted into it
+   (remove_atoms_outside_xy_range / shift_atoms, :146-157, in float as the reference's T = float),
+   and the window is simulated with the probe at its centre; an empty window records the blank
+   intensity N^2 x (aperture pixels inside the detector).  Configurations are summed with their
+   weights (the reference assigns each over the previous one). */
+static int or_simulate_stem_general(const ms_params* p, const ms_atoms* a, double* stem)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    int c0, c1;
+    double w;
+    or_confs(p, &c0, &c1, &w);
+    int npos = p->scan_nx * p->scan_ny;
+    memset(stem, 0, sizeof(double) * (size_t)p->n_det * npos);
+    double blank[MS_MAX_DET];
+    {
+        or_lens L;
+        or_lens_init(&p->cond_lens, s.lambda, 0.0, &L);
+        for (int d = 0; d < p->n_det; d++) {
+            float gi = or_g2_thr(p->det_inner[d], s.lambda), go = or_g2_thr(p->det_outer[d], s.lambda);
+            double cnt = 0.0;
+            for (int iy = 0; iy < s.ny; iy++)
+                for (int ix = 0; ix < s.nx; ix++) {
+                    float g2 = or_g2f(&s, ix, iy);
+                    if (L.g2min <= g2 && g2 < L.g2max && gi <= g2 && g2 <= go) cnt += 1.0;
+                }
+            blank[d] = cnt * (double)s.N * (double)s.N;
+        }
+    }
+    int64_t n = a->n;
+    float* xd = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* yd = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* zd = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    int* cZ = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    float* cx = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* cy = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* cz = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* cs = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    float* co = (float*)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    ms_params q = *p;
+    q.phonon_model = MS_PHONON_STILL;
+    q.pn_nconf = 1;
+    q.exec_mode = MS_EXEC_BATCHED;
+    q.scan_nx = q.scan_ny = 1;
+    q.scan_x0 = 0.5 * p->lx;
+    q.scan_y0 = 0.5 * p->ly;
+    q.scan_dx = q.scan_dy = 0.0;
+    double Id[MS_MAX_DET];
+    for (int c = c0; c <= c1; c++) {
+        or_displace(p, a, c, xd, yd, zd);
+        for (int ip = 0; ip < npos; ip++) {
+            int ix = ip % p->scan_nx, iy = ip / p->scan_nx;
+            double px = p->scan_x0 + ix * p->scan_dx, py = p->scan_y0 + iy * p->scan_dy;
+            float xs = (float)(px - 0.5 * p->lx), ys = (float)(py - 0.5 * p->ly);
+            float xlo = xs - 2.0f, xhi = (xs + (float)p->lx) + 2.0f;
+            float ylo = ys - 2.0f, yhi = (ys + (float)p->ly) + 2.0f;
+            int64_t m = 0;
+            for (int64_t k = 0; k < n; k++) {
+                if (xd[k] < xlo || xd[k] > xhi || yd[k] < ylo || yd[k] > yhi) continue;
+                cZ[m] = a->Z[k];
+                cx[m] = xd[k] - xs;
+                cy[m] = yd[k] - ys;
+                cz[m] = zd[k];
+                cs[m] = a->sigma ? a->sigma[k] : 0.0f;
+                co[m] = a->occ ? a->occ[k] : 1.0f;
+                m++;
+            }
+            if (m == 0) {
+                for (int d = 0; d < p->n_det; d++) stem[(size_t)d * npos + ip] += w * blank[d];
+                continue;
+            }
+            ms_atoms wa;
+            wa.n = m;
+            wa.Z = cZ;
+            wa.x = cx;
+            wa.y = cy;
+            wa.z = cz;
+            wa.sigma = cs;
+            wa.occ = co;
+            or_simulate_stem(&q, &wa, Id);
+            for (int d = 0; d < p->n_det; d++) stem[(size_t)d * npos + ip] += w * Id[d];
+        }
+    }
+    free(xd); free(yd); free(zd); free(cZ); free(cx); free(cy); free(cz); free(cs); free(co);
+    return 0;
+}
+
 /* run_STEM_tile_simu (scan_simulator.cuh:11-113) for a grid that covers the
    specimen: per configuration, store all slice potentials, then run every
    probe position and integrate each detector. */
 int or_simulate_stem(const ms_params* p, const ms_atoms* a, double* stem)
 {
+    if (p->exec_mode == MS_EXEC_GENERAL) return or_simulate_stem_general(p, a, stem);
     or_sim s;
     or_sim_init(p, &s);
     int c0, c1;
