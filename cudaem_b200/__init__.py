@@ -266,6 +266,10 @@ class Context:
         """0: classic one-block-per-tile slice passes (default); 1: persistent pipelined passes."""
         self.check(lib().ms_set_pass_kernels(self.handle, variant))
 
+    def set_fault_injection(self, what: int) -> None:
+        """Host-side fault injection for failure-path tests (abi.MS_INJECT_*)."""
+        self.check(lib().ms_set_fault_injection(self.handle, int(what)))
+
     def set_potential_overlap(self, enable: bool) -> None:
         """False: all potentials before the slice loop (default); True: 16-slice chunks on a side
         stream beside the slice passes.  Identical results."""

@@ -29,6 +29,7 @@ MS_TSI_TEMPORAL_SPATIAL, MS_TSI_TEMPORAL, MS_TSI_SPATIAL, MS_TSI_COHERENT = 1, 2
 MS_RECORD_INTENSITY, MS_RECORD_WAVE = 0, 1
 MS_EXEC_BATCHED, MS_EXEC_PLAIN, MS_EXEC_GENERAL = 0, 1, 2
 MS_BORDER_MIN, MS_BORDER_MAX, MS_BORDER_MIDDLE = 0, 1, 2
+MS_INJECT_NONE, MS_INJECT_WAIT_TIMEOUT = 0, 1
 
 
 class ms_lens(C.Structure):
@@ -127,6 +128,7 @@ PROTOTYPES = {
     "ms_profile_reset": (C.c_int, [C.c_void_p]),
     "ms_profile_get": (C.c_int, [C.c_void_p, C.c_char_p, _P(C.c_int64), _P(C.c_double)]),
     "ms_physics": (C.c_int, [C.c_double, _P(C.c_double), _P(C.c_double), _P(C.c_double)]),
+    "ms_set_fault_injection": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_simulate_tem": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), _P(ms_output)]),
     "ms_simulate_tem_defocus_series": (C.c_int, [C.c_void_p, _P(ms_params), _P(ms_atoms), C.c_int,
                                                  _P(C.c_double), _P(ms_output)]),

@@ -179,6 +179,13 @@ ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
     return MS_OK;
 }
 
+ms_status ms_set_fault_injection(ms_ctx* c, int what)
+{
+    if (!c || (what != MS_INJECT_NONE && what != MS_INJECT_WAIT_TIMEOUT)) return MS_ERR_INVALID_ARG;
+    c->inject = what;
+    return MS_OK;
+}
+
 ms_status ms_set_potential_overlap(ms_ctx* c, int enable)
 {
     if (!c) return MS_ERR_INVALID_ARG;

@@ -22,6 +22,107 @@ inline void smem_attr(F* kernel, size_t bytes)
     smem_attr_raw((const void*)kernel, bytes);
 }
 int num_sms();
+// A 2-D tensor map over a wave batch seen as rows x (2 nx) floats (rows = waves x ny), with boxes of
+// box_cols floats x box_rows rows; false when the driver cannot encode it.
+bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows);
+
+// ---------------------------------------------------------------------------
+// L2 eviction policies for the slice passes (createpolicy over the whole access) and loads /
+// stores that carry them
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t l2_policy_evict_last()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_normal()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// read-only data of the whole launch (tables, the transmission store)
+__device__ __forceinline__ float2 ld_nc_l2hint(const float2* ptr, uint64_t pol)
+{
+    float2 v;
+    asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(ptr), "l"(pol));
+    return v;
+}
+// the wave (written by the previous pass)
+__device__ __forceinline__ float2 ld_l2hint(const float2* ptr, uint64_t pol)
+{
+    float2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(ptr), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_l2hint(float2* ptr, float2 v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(ptr), "f"(v.x), "f"(v.y), "l"(pol)
+                 : "memory");
+}
+// Policy of the wave batch's stores and of the transmission loads of one pass (PassArgs.l2_mode):
+// L2_WAVES_RESIDENT keeps the batch's waves in L2 between the passes and streams the transmission;
+// L2_SHARED_T keeps the transmission (read by every wave of the batch) and streams the waves.
+__device__ __forceinline__ uint64_t l2_policy_wave(int mode)
+{
+    return mode == L2_WAVES_RESIDENT ? l2_policy_evict_last()
+                                     : (mode == L2_SHARED_T ? l2_policy_evict_first() : l2_policy_evict_normal());
+}
+__device__ __forceinline__ uint64_t l2_policy_trans(int mode)
+{
+    return mode == L2_WAVES_RESIDENT ? l2_policy_evict_first()
+                                     : (mode == L2_SHARED_T ? l2_policy_evict_last() : l2_policy_evict_normal());
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-memory-access (TMA) tile loads into shared memory, completed on an mbarrier
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `phase` of the barrier for at most `limit` clock cycles; false when the wait ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase, long long limit)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, phase))
+        if (clock64() - t0 > limit) return false;
+    return true;
+}
+// One 2-D box of the tensor map into shared memory at dst (128-byte aligned); x is the inner
+// coordinate in elements (its byte offset a multiple of 16), y the row.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+// default limit of a device-side wait: about one second at the B200's clock
+constexpr long long kWaitCycles = 2000000000LL;
 
 // ---------------------------------------------------------------------------
 // lens phase (coherent_phase_shift, basic_functions_dev.cuh:215-234) in FP64

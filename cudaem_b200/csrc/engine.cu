@@ -86,6 +86,8 @@ void ms_ctx::release_all()
     twiddles.clear();
     if (exptab) cudaFree(exptab);
     exptab = nullptr;
+    if (d_err) cudaFree(d_err);
+    d_err = nullptr;
     prop_key.clear();
 }
 
@@ -172,24 +174,23 @@ int team_size(int N)
     throw MsError(MS_ERR_UNSUPPORTED, "unsupported transform length");
 }
 
+// Inter-level twiddles W_N^(g k1) at [k1 * G + g], in kTwSets dithered sets of N entries (set t
+// used by the slices s with s mod kTwSets = t), from FP64 values.
 const float2* twiddles(ms_ctx* c, int N)
 {
     auto it = c->twiddles.find(N);
     if (it != c->twiddles.end()) return (const float2*)it->second;
     int G = team_size(N), E = N / G;
-    std::vector<float2> t(2 * (size_t)N);  // high parts, then the rounded remainders
+    std::vector<float2> t((size_t)kTwSets * N);
     for (int k1 = 0; k1 < E; k1++)
         for (int g = 0; g < G; g++) {
             double a = -2.0 * kPi * (double)((int64_t)g * k1 % N) / (double)N;
-            double c = std::cos(a), s = std::sin(a);
-            float2 hi = make_float2((float)c, (float)s);
-            t[(size_t)k1 * G + g] = hi;
-            t[(size_t)N + k1 * G + g] = make_float2((float)(c - (double)hi.x), (float)(s - (double)hi.y));
+            dither_sets(std::cos(a), std::sin(a), kTwSets, t.data() + (size_t)k1 * G + g, (size_t)N);
         }
     void* p = nullptr;
-    CK(cudaMalloc(&p, sizeof(float2) * 2 * N));
+    CK(cudaMalloc(&p, sizeof(float2) * t.size()));
     c->forget_free_mem();
-    CK(cudaMemcpy(p, t.data(), sizeof(float2) * 2 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(p, t.data(), sizeof(float2) * t.size(), cudaMemcpyHostToDevice));
     c->twiddles[N] = p;
     return (const float2*)p;
 }
@@ -279,12 +280,14 @@ struct Setup {
     const float2* exptab;
     int64_t N;
     int variant = PASS_CLASSIC;
+    int* err = nullptr;        // the context's device wait-error word
 };
 
 Setup make_setup(ms_ctx* c, const ms_params& p)
 {
     Setup s;
     s.variant = c->pass_variant;
+    s.err = c->d_err;
     s.ph = physics_of(p.E0, p.theta);
     s.gc = grid_of(p, s.ph);
     s.N = (int64_t)p.nx * p.ny;
@@ -326,7 +329,7 @@ Setup make_setup(ms_ctx* c, const ms_params& p)
     char key[256];
     std::snprintf(key, sizeof(key), "%d,%d,%.17g,%.17g,%.17g,%.17g,%.17g,%d", p.nx, p.ny, p.lx, p.ly, s.gc.prop_w,
                   s.gc.g0x, s.gc.g0y, p.bwl);
-    float2* P = (float2*)c->buf("prop", sizeof(float2) * s.N);
+    float2* P = (float2*)c->buf("prop", sizeof(float2) * kPropSets * s.N);   // dithered tables
     if (c->prop_key != key) {
         launch_prop_table(p.nx, p.ny, s.gc.dgx, s.gc.dgy, s.gc.g0x, s.gc.g0y, s.gc.prop_w, s.gc.alpha, s.gc.gl2,
                           p.bwl ? 1 : 0, P, c->stream);
@@ -690,17 +693,34 @@ PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const flo
     a.grid = s.gd;
     a.lens = lens;
     a.variant = s.variant;
+    a.err = s.err;
     return a;
 }
 
+// The waves of a batch stay in L2 between the passes (evict-last) when they take at most 72 MiB of
+// the 126 MB L2 next to the 16 MiB propagator table; the transmission slices then stream through.
+int l2_mode_for_waves(int nwaves, int64_t N)
+{
+    return (double)nwaves * (double)N * sizeof(float2) <= 72.0 * 1024 * 1024 ? L2_WAVES_RESIDENT : L2_DEFAULT;
+}
+
+// Device time and launches of one call; the context's wait-error word is cleared at the start and
+// read at the end (a kernel whose bounded wait ran out has set it).
 struct Timer {
     ms_ctx* c;
     int64_t l0;
-    explicit Timer(ms_ctx* cc) : c(cc), l0(kernel_launches()) { CK(cudaEventRecord(c->ev0, c->stream)); }
+    explicit Timer(ms_ctx* cc) : c(cc), l0(kernel_launches())
+    {
+        CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+        CK(cudaEventRecord(c->ev0, c->stream));
+    }
     void stop()
     {
         CK(cudaEventRecord(c->ev1, c->stream));
         CK(cudaEventSynchronize(c->ev1));
+        int e = 0;
+        CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) throw MsError(MS_ERR_TIMEOUT, "a device-side wait for a shared-memory tile ran out");
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
         c->last_ms = ms;
@@ -743,7 +763,15 @@ size_t fine_bytes_per_conf(const ms_params& p, const ms_atoms& a)
 
 }  // namespace
 
-void ctx_activate(ms_ctx* c) { CK(cudaSetDevice(c->device)); }
+void ctx_activate(ms_ctx* c)
+{
+    CK(cudaSetDevice(c->device));
+    if (!c->d_err) {
+        CK(cudaMalloc(&c->d_err, sizeof(int)));
+        c->forget_free_mem();
+        CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    }
+}
 
 // ---------------------------------------------------------------------------
 // HRTEM / ED (ED_HRTEM, single_simulator.cuh:11-126) and CBED (CBED_CBEI, :128-206)
@@ -817,6 +845,7 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nw, cudaMemcpyHostToDevice, st));
         float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * nw);
         PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
+        pa.l2_mode = l2_mode_for_waves(nw, N);
         pa.tt = sT;
         if (iw == MS_IW_CONVERGENT) {
             pa.tw = s.tw_y;
@@ -832,7 +861,9 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
             if (sl == 0 && iw == MS_IW_PLANE_TILTED) pr.flags |= PF_TILT_INCIDENT;
             run_row(c, p.nx, (sl == 0 && plane) ? ROW_T_FWD : ROW_INV_T_FWD, pr, nw, p.ny, st);
             pa.tw = s.tw_y;
-            run_col(c, p.ny, COL_STEP, pa, nw, p.nx, st);
+            PassArgs pc = pa;
+            if (c->inject == MS_INJECT_WAIT_TIMEOUT) pc.flags |= PF_TEST_WAIT;
+            run_col(c, p.ny, COL_STEP, pc, nw, p.nx, st);
         }
         const int illum = p.illumination_model ? p.illumination_model : MS_ILLUM_COHERENT;
         const int tsi = p.temporal_spatial_incoh ? p.temporal_spatial_incoh : MS_TSI_TEMPORAL_SPATIAL;
@@ -1304,6 +1335,7 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
             const int nb = std::min(B, npos - start);
             CK(cudaMemcpyAsync(dwv, dwv_all + start, sizeof(WaveInfo) * nb, cudaMemcpyDeviceToDevice, st));
             PassArgs pa = pass_args(s, psi, dwv, nullptr, plain ? 0 : slot, cond);
+            pa.l2_mode = plain ? L2_DEFAULT : L2_SHARED_T;   // one transmission slice serves the whole batch
             pa.tt = sT;
             if (!plain) {
                 auto body = [&] {
@@ -1415,6 +1447,7 @@ void sim_thickness(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* 
         float2* psi = (float2*)c->buf("psi", sizeof(float2) * N);
         float2* aux = (float2*)c->buf("aux", sizeof(float2) * N);
         PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
+        pa.l2_mode = l2_mode_for_waves(1, N);
         pa.tt = sT;
         pa.aux = aux;
         pa.filt_g2in = g2in;
@@ -1861,7 +1894,7 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             const int64_t slot = (int64_t)g.S_cap * N;
             I.sV = (float*)take("many_sV_" + std::to_string(i), sizeof(float) * slot * g.nconf);
             run_potential(c, pot_args(p, s0, A, g, I.sV, slot, 0, g.S_cap, 0), g.nconf, st);
-            I.prop = (float2*)take("many_prop_" + std::to_string(i), sizeof(float2) * N);
+            I.prop = (float2*)take("many_prop_" + std::to_string(i), sizeof(float2) * kPropSets * N);
             launch_prop_table(p.nx, p.ny, gc.dgx, gc.dgy, gc.g0x, gc.g0y, gc.prop_w, gc.alpha, gc.gl2, p.bwl ? 1 : 0,
                               I.prop, st);
             I.out = (float*)take("many_out_" + std::to_string(i), sizeof(float) * N);
@@ -1962,6 +1995,7 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
                 pa.slice = sl;
                 pa.exptab = ex;
                 pa.grid = in[G.inst.front()].gd;
+                pa.err = c->d_err;
                 pa.tw = twiddles(c, G.nx);
                 launch_row(G.nx, ROW_INV_T_FWD, pa, nact, G.ny, G.s);
                 pa.tw = twiddles(c, G.ny);

@@ -21,15 +21,6 @@
 
 #include "fft_layout.hpp"
 
-// Twiddle precision: 1 carries the register-DFT constants (MS_SPLIT_REG) and the inter-level
-// twiddles (MS_SPLIT_LEVEL) as hi + lo float pairs, 0 as one float.
-#ifndef MS_SPLIT_REG
-#define MS_SPLIT_REG 1
-#endif
-#ifndef MS_SPLIT_LEVEL
-#define MS_SPLIT_LEVEL 1
-#endif
-
 namespace msb {
 
 // W_64^m = exp(-2 pi i m / 64) as an unevaluated sum hi + lo of two floats: hi is the double
@@ -140,7 +131,7 @@ __device__ __forceinline__ float2 tw_apply(float2 d, int m)
     if (m == 8 || m == 24) {
         // W_64^8 = (1 - i)/sqrt2 and W_64^24 = (-1 - i)/sqrt2 (their conjugates for DIR > 0): a sum
         // and a difference of the two parts, each scaled by 1/sqrt2 carried as hi + lo
-        const float hs = c_tw64[8].x, ls = MS_SPLIT_REG ? c_tw64_lo[8].x : 0.0f;
+        const float hs = c_tw64[8].x, ls = c_tw64_lo[8].x;
         float re, im;
         if (DIR < 0) {
             re = (m == 8) ? d.x + d.y : d.y - d.x;
@@ -151,7 +142,6 @@ __device__ __forceinline__ float2 tw_apply(float2 d, int m)
         }
         return make_float2(fmaf(re, hs, re * ls), fmaf(im, hs, im * ls));
     }
-    if (!MS_SPLIT_REG) return DIR < 0 ? cmul(d, c_tw64[m]) : cmulc(d, c_tw64[m]);
     return DIR < 0 ? cmul_split(d, c_tw64[m], c_tw64_lo[m]) : cmulc_split(d, c_tw64[m], c_tw64_lo[m]);
 }
 
@@ -187,8 +177,8 @@ __device__ __forceinline__ void dft_reg(float2 (&a)[E])
 }
 
 // Team transform.  On entry v[j] = x[g + G j]; on exit v[j] = X[g + G j].
-// `tw` is the shared table W_N^(g k1) at tw[k1 * G + g] (high parts) followed by the
-// low parts at tw[N + k1 * G + g].  `scr(k1, g)` returns
+// `tw` is the shared table W_N^(g k1) at tw[k1 * G + g] (one of the dithered sets: the
+// engine's slices take the sets in turn, see kTwSets).  `scr(k1, g)` returns
 // the shared-memory slot for the transpose; `sync()` orders the team's shared
 // accesses (a warp barrier when the team is inside one warp, a block barrier
 // otherwise).
@@ -201,13 +191,8 @@ __device__ __forceinline__ void team_fft(float2 (&v)[N / G], int g, const float2
     dft_reg<E, DIR>(v);
 #pragma unroll
     for (int k1 = 1; k1 < E; k1++) {
-        const float2 wh = tw[k1 * G + g];
-        if (!MS_SPLIT_LEVEL) {
-            v[brev<E>(k1)] = DIR < 0 ? cmul(v[brev<E>(k1)], wh) : cmulc(v[brev<E>(k1)], wh);
-            continue;
-        }
-        const float2 wl = tw[N + k1 * G + g];
-        v[brev<E>(k1)] = DIR < 0 ? cmul_split(v[brev<E>(k1)], wh, wl) : cmulc_split(v[brev<E>(k1)], wh, wl);
+        const float2 w = tw[k1 * G + g];
+        v[brev<E>(k1)] = DIR < 0 ? cmul(v[brev<E>(k1)], w) : cmulc(v[brev<E>(k1)], w);
     }
     sync();
 #pragma unroll

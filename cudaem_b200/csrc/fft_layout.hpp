@@ -5,6 +5,35 @@
 
 namespace msb {
 
+// Dithered tables of the operators that every slice repeats.  The inter-level FFT twiddles
+// (kTwSets sets) and the propagator P(k) (kPropSets tables) are each rounded to float in several
+// versions, and slice s uses version s mod K.  The versions follow sigma-delta rounding: version t
+// is the float nearest to (t + 1) w minus the sum of versions 0..t-1, so the running sum over
+// consecutive slices stays within half an ulp of the exact multiple of w.  A single rounded table
+// would repeat the same rounding error at every slice; its effect on the wave adds up coherently
+// over a thick specimen (at 240 slices the propagator's rounding alone costs about 5e-6 relative).
+constexpr int kTwSets = 8;
+constexpr int kPropSets = 8;
+
+#ifdef __CUDACC__
+#define MS_FL_HD __host__ __device__
+#else
+#define MS_FL_HD
+#endif
+// Versions t = 0..K-1 of the complex value (re, im), written to out[t * stride].
+template <class F2>
+MS_FL_HD inline void dither_sets(double re, double im, int K, F2* out, size_t stride)
+{
+    double sr = 0.0, si = 0.0;
+    for (int t = 0; t < K; t++) {
+        const float vr = (float)((t + 1) * re - sr), vi = (float)((t + 1) * im - si);
+        sr += (double)vr;
+        si += (double)vi;
+        out[(size_t)t * stride].x = vr;
+        out[(size_t)t * stride].y = vi;
+    }
+}
+
 // Per-size layout of the passes.
 //   G: threads per transform; E = N/G points per thread.
 //   ROWS: transforms per block in the row pass (one team each, inside a warp).
@@ -49,9 +78,9 @@ struct FftLayout {
     static constexpr int SCR_STRIDE_ROW = SCR_BASE + 1;
     static constexpr int SCR_STRIDE_COL =
         (TC == 16) ? (SCR_BASE + ((1 - SCR_BASE % 16) + 16) % 16) : (SCR_BASE + ((2 - SCR_BASE % 16) + 16) % 16);
-    // transpose scratch, twiddles (high and low parts), and the 1024-entry exp(i phi) table
-    static constexpr size_t ROW_SMEM = sizeof(float2) * ((size_t)ROWS * SCR_STRIDE_ROW + 2 * N + 1024);
-    static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + (COL_TW_GLOBAL ? 0 : 2 * N));
+    // transpose scratch, one set of twiddles, and the 1024-entry exp(i phi) table
+    static constexpr size_t ROW_SMEM = sizeof(float2) * ((size_t)ROWS * SCR_STRIDE_ROW + N + 1024);
+    static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + (COL_TW_GLOBAL ? 0 : N));
 };
 
 }  // namespace msb

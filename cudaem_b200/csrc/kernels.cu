@@ -2,6 +2,8 @@
 // table, the projected potential, the specimen pipeline (displacement, slicing, sort, gather),
 // fine slicing, detectors, accumulation and output, and the adjoint's helpers.
 #include <cub/device/device_radix_sort.cuh>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -43,6 +45,30 @@ void smem_attr_raw(const void* kernel, size_t bytes)
     g_attr_max[key] = bytes;
 }
 
+// cuTensorMapEncodeTiled, looked up once through the runtime's driver entry points (the library
+// does not link the driver library).
+bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = (PFN_cuTensorMapEncodeTiled_v12000)f;
+        cudaGetLastError();
+    });
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)2 * nx, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)2 * nx * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode((CUtensorMap*)map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(psi), dims, strides, box,
+                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 void check_launch(const char* what)
 {
     cudaError_t e = cudaGetLastError();
@@ -63,7 +89,9 @@ int num_sms()
     return n[dev];
 }
 
-// Full propagator table in FP64, rounded to FP32 (gen_propagator_kernel, device_kernels.cuh:215-234)
+// Full propagator table in FP64 (gen_propagator_kernel, device_kernels.cuh:215-234), rounded to
+// kPropSets dithered FP32 tables (fft_layout.hpp): P holds kPropSets * nx * ny entries, table t
+// used by the slices s with s mod kPropSets = t.
 __global__ void k_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
                              double gl2, int bwl, double inv_n, float2* P)
 {
@@ -75,7 +103,7 @@ __global__ void k_prop_table(int nx, int ny, double dgx, double dgy, double g0x,
     double th = w * ((gx - g0x) * (gx - g0x) + (gy - g0y) * (gy - g0y));
     double s, c;
     sincos(th, &s, &c);
-    P[(size_t)iy * nx + ix] = make_float2((float)(amp * c), (float)(amp * s));
+    dither_sets(amp * c, amp * s, kPropSets, P + (size_t)iy * nx + ix, (size_t)nx * ny);
 }
 
 void launch_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,

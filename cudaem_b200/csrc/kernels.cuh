@@ -16,7 +16,7 @@ struct WaveInfo {
     float weight = 1.0f;         // configuration weight
     int pos = 0;                 // output index (scan position) of the wave
     const float* sV = nullptr;      // if set: this wave's own potential store [slice][ny][nx] (uneven batches)
-    const float2* prop = nullptr;   // if set: this wave's own propagator table [ny][nx]
+    const float2* prop = nullptr;   // if set: this wave's own propagator table [2][ny][nx] (hi, lo planes)
 };
 
 struct GridDev {
@@ -71,7 +71,8 @@ enum PassFlags {
     PF_STORE_X = 16,       // ROW_INV_T_FWD also writes the transmitted real-space wave to xs
     PF_CONJ_PROP = 32,     // COL_STEP multiplies by conj(P) (the adjoint step)
     PF_WAVE_DEFOCUS = 64,  // COL_CTF_INV takes each wave's own defocus term (WaveInfo.cc10) instead of the lens's
-    PF_TILT_INCIDENT = 128 // ROW_T_FWD / ROW_TT_FWD start from the tilted plane wave exp(2 pi i g0.(r - L/2))
+    PF_TILT_INCIDENT = 128, // ROW_T_FWD / ROW_TT_FWD start from the tilted plane wave exp(2 pi i g0.(r - L/2))
+    PF_TEST_WAIT = 256      // fault injection: the TMA column pass waits for bytes that never come
 };
 
 struct PassArgs {
@@ -88,7 +89,7 @@ struct PassArgs {
     const float2* tw;         // inter-level twiddles for this pass's length
     const float2* prop_x;     // [nx] exp(i w (gx - g0x)^2)
     const float2* prop_y;     // [ny] exp(i w (gy - g0y)^2)
-    const float2* prop;       // [ny][nx] full propagator P(k) including 1/N and the band limit
+    const float2* prop;       // [2][ny][nx] full propagator P(k) including 1/N and the band limit, as hi + lo planes
     const float2* exptab;     // [1024] exp(2 pi i k / 1024) for the transmission
     GridDev grid;
     LensDev lens;
@@ -101,6 +102,16 @@ struct PassArgs {
     int ndet;
     double* chi_part;         // [B][nx / TC][2] partial sums of g^2 q and g^4 q
     int variant;              // PassVariant of the row / column pass kernels (host side only)
+    int l2_mode;              // L2Mode: eviction priorities of the wave and transmission accesses
+    int* err;                 // device word set to a nonzero code when a bounded device-side wait runs out
+    long long wait_cycles;    // limit of such a wait in clock cycles (0: about one second)
+};
+
+// L2 eviction priorities of the slice passes' wave stores and transmission loads.
+enum L2Mode {
+    L2_DEFAULT = 0,         // no priority
+    L2_WAVES_RESIDENT = 1,  // the batch's waves fit in L2: waves evict-last, transmission evict-first
+    L2_SHARED_T = 2         // one transmission slice serves every wave: transmission evict-last, waves evict-first
 };
 
 // Kernel form of ROW_INV_T_FWD and COL_STEP: the classic one-block-per-tile kernels (two

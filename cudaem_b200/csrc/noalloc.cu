@@ -45,8 +45,8 @@ constexpr int kMaxBatch = 256;
 constexpr int kMaxN = 2048;
 constexpr int kMaxBlk = 64;
 constexpr int kExpN = 1024;
-// tw_x and tw_y (high then low parts, 2 kMaxN each), prop_x, prop_y, exp table
-constexpr size_t kTableBytes = sizeof(float2) * (6 * kMaxN + kExpN);
+// tw_x and tw_y (kTwSets dithered sets each), prop_x, prop_y, exp table
+constexpr size_t kTableBytes = sizeof(float2) * (2 * (size_t)kTwSets * kMaxN + 2 * kMaxN + kExpN);
 constexpr size_t kWaveInfoBytes = sizeof(WaveInfo) * kMaxBatch;
 constexpr size_t kThrBytes = 256;                                                     // 2 * MS_MAX_DET floats
 constexpr size_t kIwaveBytes = sizeof(double) * kMaxBatch * MS_MAX_DET;
@@ -143,18 +143,15 @@ int team_size_of(int N)
     throw MsError(MS_ERR_UNSUPPORTED, "unsupported transform length");
 }
 
+// the kTwSets dithered sets of the inter-level twiddles, set t at out[t * N]
 void twiddle_table(int N, float2* out)
 {
-    // high parts at out[0, N), rounded remainders at out[N, 2N)
     const double pi = 3.14159265358979323846264338327950288;
     int G = team_size_of(N), E = N / G;
     for (int k1 = 0; k1 < E; k1++)
         for (int g = 0; g < G; g++) {
             double a = -2.0 * pi * (double)((int64_t)g * k1 % N) / (double)N;
-            double c = std::cos(a), s = std::sin(a);
-            float2 hi = make_float2((float)c, (float)s);
-            out[(size_t)k1 * G + g] = hi;
-            out[(size_t)N + k1 * G + g] = make_float2((float)(c - (double)hi.x), (float)(s - (double)hi.y));
+            dither_sets(std::cos(a), std::sin(a), kTwSets, out + (size_t)k1 * G + g, (size_t)N);
         }
 }
 
@@ -186,8 +183,8 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
         DevState& ds = setup_current_device();
         base = ds.addr;
         float2* tw_x = (float2*)(base + kOffTables);
-        float2* tw_y = tw_x + 2 * kMaxN;
-        float2* prop_x = tw_y + 2 * kMaxN;
+        float2* tw_y = tw_x + (size_t)kTwSets * kMaxN;
+        float2* prop_x = tw_y + (size_t)kTwSets * kMaxN;
         float2* prop_y = prop_x + kMaxN;
         float2* exptab = prop_y + kMaxN;
         const TableKey key{p.nx, p.ny, gc.dgx, gc.dgy, gc.g0x, gc.g0y, gc.prop_w};
@@ -201,12 +198,12 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
             ck(cudaMemcpyAsync(exptab, et.data(), sizeof(float2) * kExpN, cudaMemcpyHostToDevice, st), "table upload");
         }
         if (!ds.have_tables || std::memcmp(&key, &ds.key, sizeof(key)) != 0) {
-            // only the entries this grid uses: 2 nx + 2 ny twiddles, nx + ny propagator factors
+            // only the entries this grid uses: kTwSets (nx + ny) twiddles, nx + ny propagator factors
             ds.have_tables = false;
-            std::vector<float2> tab(3 * (size_t)(p.nx + p.ny));
+            std::vector<float2> tab((size_t)(kTwSets + 1) * (p.nx + p.ny));
             float2* tx = tab.data();
-            float2* ty = tx + 2 * p.nx;
-            float2* px = ty + 2 * p.ny;
+            float2* ty = tx + (size_t)kTwSets * p.nx;
+            float2* px = ty + (size_t)kTwSets * p.ny;
             float2* py = px + p.nx;
             twiddle_table(p.nx, tx);
             twiddle_table(p.ny, ty);
@@ -220,8 +217,8 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
                 double th = gc.prop_w * g * g;
                 py[i] = make_float2((float)std::cos(th), (float)std::sin(th));
             }
-            ck(cudaMemcpyAsync(tw_x, tx, sizeof(float2) * 2 * p.nx, cudaMemcpyHostToDevice, st), "table upload");
-            ck(cudaMemcpyAsync(tw_y, ty, sizeof(float2) * 2 * p.ny, cudaMemcpyHostToDevice, st), "table upload");
+            ck(cudaMemcpyAsync(tw_x, tx, sizeof(float2) * kTwSets * p.nx, cudaMemcpyHostToDevice, st), "table upload");
+            ck(cudaMemcpyAsync(tw_y, ty, sizeof(float2) * kTwSets * p.ny, cudaMemcpyHostToDevice, st), "table upload");
             ck(cudaMemcpyAsync(prop_x, px, sizeof(float2) * p.nx, cudaMemcpyHostToDevice, st), "table upload");
             ck(cudaMemcpyAsync(prop_y, py, sizeof(float2) * p.ny, cudaMemcpyHostToDevice, st), "table upload");
             ds.key = key;
@@ -229,8 +226,8 @@ void stem_forward_noalloc(cudaStream_t st, const ms_params& p, const float* V, i
         }
     }
     float2* tw_x = (float2*)(base + kOffTables);
-    float2* tw_y = tw_x + 2 * kMaxN;
-    float2* prop_x = tw_y + 2 * kMaxN;
+    float2* tw_y = tw_x + (size_t)kTwSets * kMaxN;
+    float2* prop_x = tw_y + (size_t)kTwSets * kMaxN;
     float2* prop_y = prop_x + kMaxN;
     float2* exptab = prop_y + kMaxN;
     WaveInfo* dwv = (WaveInfo*)(base + kOffWaveInfo);

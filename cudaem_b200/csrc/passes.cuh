@@ -10,6 +10,8 @@
 // HRTEM column pass.  Every transform length is compiled in its own translation
 // unit (passes_<N>.cu), which instantiates row_dispatch<N> and col_dispatch<N>.
 #pragma once
+#include <cuda.h>
+
 #include <algorithm>
 #include <cstdint>
 
@@ -19,6 +21,18 @@
 #include "kernels.cuh"
 
 namespace msb {
+
+// The twiddle set of this launch's slice (kTwSets dithered sets of N entries at a.tw).
+template <int N>
+__device__ __forceinline__ const float2* tw_set(const PassArgs& a)
+{
+    return a.tw + (size_t)((unsigned)a.slice % (unsigned)kTwSets) * N;
+}
+// The propagator table of this launch's slice: kPropSets dithered tables of nx*ny entries.
+__device__ __forceinline__ const float2* prop_set(const float2* base, const PassArgs& a)
+{
+    return base + (size_t)((unsigned)a.slice % (unsigned)kPropSets) * ((size_t)a.grid.nx * a.grid.ny);
+}
 
 // ---------------------------------------------------------------------------
 template <int N, int OP>
@@ -47,8 +61,8 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
         for (int j = 0; j < E; j++) v[j] = a.psi[row_off + g + G * j];
     }
     float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
-    float2* etab = tw + 2 * N;
-    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tw[i] = a.tw[i];
+    float2* etab = tw + N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_set<N>(a)[i];
     if ((kT && !kTT) || OP == ROW_ADJ)
         for (int i = threadIdx.x; i < kExpTab; i += blockDim.x) etab[i] = a.exptab[i];
     __syncthreads();
@@ -132,6 +146,57 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
     }
 }
 
+// Row pass on a transmission store (ROW_INV_TT_FWD), the hot pass of the CBED, HRTEM, STEM and
+// thickness loops: inverse row FFT, times t, forward row FFT, one row per warp.  A lean copy of
+// k_row's path: only the wave's slice count and configuration slot are read from its descriptor,
+// and the addresses are formed where they are used, so nothing stays live across the transforms
+// but the row's values (k_row's general form spills here).  Loads and stores carry the L2
+// eviction priorities of PassArgs.l2_mode, a template argument MODE (a policy chosen at run time
+// costs the registers that make the kernel spill).
+template <int N, int MODE>
+__global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_MINB) k_row_tt(PassArgs a)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E;
+    extern __shared__ float2 smem[];
+    const int ny = a.grid.ny;
+    const int blocks_per_wave = ny / L::ROWS;
+    const int b = blockIdx.x / blocks_per_wave;
+    const int team = threadIdx.x / G, g = threadIdx.x % G;
+    const int r = (blockIdx.x % blocks_per_wave) * L::ROWS + team;
+    const bool beyond = a.slice >= a.waves[b].n_slices;
+    if (beyond && !(a.flags & PF_VACUUM_BEYOND)) return;
+    float2 v[E];
+    {
+        const float2* src = a.psi + ((size_t)b * ny + r) * N + g;
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = src[G * j];
+    }
+    float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_set<N>(a)[i];
+    __syncthreads();
+    float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncwarp(); };
+    // inverse row FFT as conj(FFT(conj(x)))
+    conj_all(v);
+    team_fft<N, G, -1>(v, g, tw, scr, sync);
+    conj_all(v);
+    if (!beyond) {
+        const int slot = opaque(a.waves + b)->conf_slot;
+        const float2* tr = opaque(a.tt) + (size_t)slot * a.sV_slot_stride +
+                           ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N + g;
+        const uint64_t pol = l2_policy_trans(MODE);
+#pragma unroll
+        for (int j = 0; j < E; j++) v[j] = cmul(v[j], ld_nc_l2hint(tr + G * j, pol));
+    }
+    team_fft<N, G, -1>(v, g, tw, scr, sync);
+    float2* dst = opaque(a.psi) + ((size_t)b * ny + r) * N + g;
+    const uint64_t pol = l2_policy_wave(MODE);
+#pragma unroll
+    for (int j = 0; j < E; j++) st_l2hint(dst + G * j, v[j], pol);
+}
+
 // ---------------------------------------------------------------------------
 // column pass
 // ---------------------------------------------------------------------------
@@ -171,7 +236,7 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
         tw = a.tw;   // read through L1: shared memory is kept for the transposes of three blocks per SM
     } else {
         float2* tws = smem + TC * L::SCR_STRIDE_COL;
-        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) tws[i] = a.tw[i];
+        for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = tw_set<N>(a)[i];
         __syncthreads();
         tw = tws;
     }
@@ -216,13 +281,16 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
                 // tabulated once per grid in FP64 and rounded to FP32; shared by every wave, so it stays in L2.
                 // The barrier keeps the table loads after the transform, so they do not hold registers
                 // across it.
-                const float2* pp = opaque((wi.prop ? wi.prop : a.prop) + (size_t)g * nx + col);
+                // The slice's dithered table, read through L2 with the evict-last policy: every wave of
+                // the launch reads it.
+                const float2* pp = opaque(prop_set(wi.prop ? wi.prop : a.prop, a) + (size_t)g * nx + col);
+                const uint64_t pl = l2_policy_evict_last();
                 if (a.flags & PF_CONJ_PROP) {
 #pragma unroll
-                    for (int j = 0; j < E; j++) v[j] = cmulc(v[j], __ldg(pp + j * cs));
+                    for (int j = 0; j < E; j++) v[j] = cmulc(v[j], ld_nc_l2hint(pp + j * cs, pl));
                 } else {
 #pragma unroll
-                    for (int j = 0; j < E; j++) v[j] = cmul(v[j], __ldg(pp + j * cs));
+                    for (int j = 0; j < E; j++) v[j] = cmul(v[j], ld_nc_l2hint(pp + j * cs, pl));
                 }
             } else {
                 // P formed per element from the separable FP64-rounded phase factors and the band limit
@@ -341,8 +409,112 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
         return;
     }
     cp = opaque(cp);
+    if constexpr (OP == COL_STEP) {
+        // the propagated wave goes on to the next row pass
+        const uint64_t pol = l2_policy_wave(a.l2_mode);
 #pragma unroll
-    for (int j = 0; j < E; j++) cp[j * cs] = v[j];
+        for (int j = 0; j < E; j++) st_l2hint(cp + j * cs, v[j], pol);
+    } else {
+#pragma unroll
+        for (int j = 0; j < E; j++) cp[j * cs] = v[j];
+    }
+    }
+}
+
+// Column step (COL_STEP) with the wave tile brought in by the tensor memory accelerator: one
+// thread issues the 2-D box loads of the block's N x TC tile into shared memory (N / 256 boxes of
+// TC columns), the block stages its twiddles meanwhile, and every thread then reads its column
+// elements from shared memory (a warp reads whole row segments: no bank conflicts).  The tile
+// region is the transposition scratch of the transforms that follow, so the block needs no more
+// shared memory than the classic kernel.  Compared with one 8-byte load per element and thread,
+// the copy engine moves the tile in large requests and leaves the load/store unit free.  The wait
+// for the tile is bounded (PassArgs.wait_cycles): when it runs out the block records the failure
+// in PassArgs.err and returns.  The arithmetic is k_col's COL_STEP.
+template <int N>
+__global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_MINB)
+    k_col_step_tma(PassArgs a, const __grid_constant__ CUtensorMap tmap)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E, TC = L::TC;
+    constexpr int BOX = N < 256 ? N : 256;
+    constexpr unsigned TILE_BYTES = (unsigned)(N * TC * sizeof(float2));
+    static_assert((size_t)TILE_BYTES <= TC * L::SCR_STRIDE_COL * sizeof(float2), "the tile lives in the scratch");
+    __shared__ __align__(8) uint64_t bar;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // 128-byte aligned base (the launch adds 128 bytes of slack)
+    float2* smem = reinterpret_cast<float2*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
+    const int nx = a.grid.nx;
+    const int tiles = nx / TC;
+    const int b = blockIdx.x / tiles;
+    const int col0 = (blockIdx.x % tiles) * TC;
+    const int c = threadIdx.x % TC, g = threadIdx.x / TC;
+    const int col = col0 + c;
+    const WaveInfo& wi = a.waves[b];
+    if (a.slice >= wi.n_slices && !(a.flags & PF_VACUUM_BEYOND)) return;
+    const bool final_step = (a.slice == wi.n_slices - 1) && !(a.flags & PF_PROP_ALWAYS);
+    float2* tile = smem;
+    float2* tws = smem + TC * L::SCR_STRIDE_COL;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, TILE_BYTES + ((a.flags & PF_TEST_WAIT) ? 16u : 0u));
+#pragma unroll
+        for (int q = 0; q < N / BOX; q++) tma_load_2d(tile + q * BOX * TC, &tmap, 2 * col0, b * N + q * BOX, &bar);
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = tw_set<N>(a)[i];
+    __syncthreads();
+    const long long limit = (a.flags & PF_TEST_WAIT) ? 2000000LL : (a.wait_cycles > 0 ? a.wait_cycles : kWaitCycles);
+    const bool late = !mbar_wait_bounded(&bar, 0, limit);
+    if (__syncthreads_or(late)) {
+        if (threadIdx.x == 0 && a.err) atomicOr(a.err, 1);
+        return;
+    }
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j] = tile[(g + G * j) * TC + c];
+    __syncthreads();   // every thread holds its values: the tile region becomes the scratch
+    float2* scr_base = smem + c * L::SCR_STRIDE_COL;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncthreads(); };
+    const size_t cs = (size_t)G * nx;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+        team_fft<N, G, -1>(v, g, tws, scr, sync);
+        if (pass == 1) {
+            conj_all(v);
+            break;
+        }
+        if (final_step) break;
+        const float2* pp = opaque(prop_set(wi.prop ? wi.prop : a.prop, a) + (size_t)g * nx + col);
+        const uint64_t pl = l2_policy_evict_last();
+        if (a.flags & PF_CONJ_PROP) {
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = cmulc(v[j], ld_nc_l2hint(pp + j * cs, pl));
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = cmul(v[j], ld_nc_l2hint(pp + j * cs, pl));
+        }
+        conj_all(v);
+    }
+    float2* cp = opaque(a.psi + (size_t)b * N * nx + (size_t)g * nx + col);
+    const uint64_t pol = l2_policy_wave(a.l2_mode);
+#pragma unroll
+    for (int j = 0; j < E; j++) st_l2hint(cp + j * cs, v[j], pol);
+}
+
+template <int N>
+static bool col_step_tma(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
+{
+    if constexpr (N < 256) {
+        return false;
+    } else {
+        using L = FftLayout<N>;
+        if (((uintptr_t)a.psi & 15) != 0) return false;
+        CUtensorMap map;
+        if (!encode_wave_tile_map(&map, a.psi, nx, (int64_t)nwaves * N, 2 * L::TC, N < 256 ? N : 256)) return false;
+        const size_t sm = L::COL_SMEM + 128;
+        smem_attr(k_col_step_tma<N>, sm);
+        k_col_step_tma<N><<<(unsigned)(nwaves * (nx / L::TC)), L::COL_THREADS, sm, st>>>(a, map);
+        return true;
     }
 }
 
@@ -377,13 +549,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_row_p(PassArgs a, int nwave
     constexpr int WARPS = kPipeThreads / 32;
     constexpr int VROW = R * N;                     // potential floats of one item
     // cp.async destinations must sit on 16-byte boundaries
-    static_assert(((WARPS * R * L::SCR_STRIDE_ROW + 2 * N + kExpTab) * sizeof(float2)) % 16 == 0, "vbuf alignment");
+    static_assert(((WARPS * R * L::SCR_STRIDE_ROW + N + kExpTab) * sizeof(float2)) % 16 == 0, "vbuf alignment");
     static_assert((VROW * sizeof(float)) % 16 == 0, "vbuf alignment");
     extern __shared__ float2 smem[];
     float2* tw = smem + WARPS * R * L::SCR_STRIDE_ROW;
-    float2* etab = tw + 2 * N;
+    float2* etab = tw + N;
     float* vbuf_all = reinterpret_cast<float*>(etab + kExpTab);   // [WARPS][2][VROW]
-    for (int i = threadIdx.x; i < 2 * N; i += kPipeThreads) tw[i] = a.tw[i];
+    for (int i = threadIdx.x; i < N; i += kPipeThreads) tw[i] = tw_set<N>(a)[i];
     for (int i = threadIdx.x; i < kExpTab; i += kPipeThreads) etab[i] = a.exptab[i];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -478,10 +650,10 @@ __global__ void __launch_bounds__(kQWarps * 32, 1) k_row_q(PassArgs a, int nwave
     constexpr int ITEM = R * N;      // float2 of one item
     extern __shared__ float2 smem[];
     float2* tw = smem;
-    for (int i = threadIdx.x; i < 2 * N; i += kQWarps * 32) tw[i] = a.tw[i];
+    for (int i = threadIdx.x; i < N; i += kQWarps * 32) tw[i] = tw_set<N>(a)[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tm = lane / G, g = lane % G;
-    float2* wbuf = smem + 2 * N + (size_t)warp * 2 * ITEM;
+    float2* wbuf = smem + N + (size_t)warp * 2 * ITEM;
     __syncthreads();
     const int ny = a.grid.ny;
     const int64_t n_items = (int64_t)nwaves * ny / R;
@@ -557,7 +729,7 @@ static bool row_q(const PassArgs& a, int nwaves, int ny, cudaStream_t st)
         constexpr int R = 32 / L::G;
         const int64_t items = (int64_t)nwaves * ny / R;
         const int64_t blocks = std::min<int64_t>((items + kQWarps - 1) / kQWarps, num_sms());
-        const size_t sm = sizeof(float2) * (2 * (size_t)N + (size_t)kQWarps * 2 * R * N);
+        const size_t sm = sizeof(float2) * ((size_t)N + (size_t)kQWarps * 2 * R * N);
         smem_attr(k_row_q<N>, sm);
         k_row_q<N><<<(unsigned)blocks, kQWarps * 32, sm, st>>>(a, nwaves);
         return true;
@@ -572,10 +744,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_col_p(PassArgs a, int nwave
     static_assert(TC * G == kPipeThreads, "the column tile must occupy the whole block");
     extern __shared__ float2 smem[];
     float2* tw = smem + TC * L::SCR_STRIDE_COL;
-    float2* ptile = tw + 2 * N;                     // propagator tile [N][TC]
-    static_assert(((TC * L::SCR_STRIDE_COL + 2 * N) * sizeof(float2)) % 16 == 0, "ptile alignment");
+    float2* ptile = tw + N;                         // propagator tile [N][TC]
+    static_assert(((TC * L::SCR_STRIDE_COL + N) * sizeof(float2)) % 16 == 0, "ptile alignment");
     static_assert(TC % 2 == 0, "16-byte propagator pieces");
-    for (int i = threadIdx.x; i < 2 * N; i += kPipeThreads) tw[i] = a.tw[i];
+    for (int i = threadIdx.x; i < N; i += kPipeThreads) tw[i] = tw_set<N>(a)[i];
     const int nx = a.grid.nx;
     const int tiles = nx / TC;
     const int64_t n_items = (int64_t)nwaves * tiles;
@@ -593,7 +765,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) k_col_p(PassArgs a, int nwave
     // the propagator tile of item `it`: N rows of TC float2, in 16-byte pieces
     auto fetch_prop = [&](int64_t it) {
         const int col0 = (int)(it % tiles) * TC;
-        const float2* P = (a.waves[(int)(it / tiles)].prop ? a.waves[(int)(it / tiles)].prop : a.prop) + col0;
+        const float2* P = prop_set(a.waves[(int)(it / tiles)].prop ? a.waves[(int)(it / tiles)].prop : a.prop, a) + col0;
         constexpr int PIECES = N * TC / 2;
         for (int q = tid; q < PIECES; q += kPipeThreads) {
             const int row = q / (TC / 2), part = q % (TC / 2);
@@ -680,7 +852,7 @@ static bool row_pipe(const PassArgs& a, int nwaves, int ny, cudaStream_t st)
         constexpr int R = 32 / L::G;
         const int64_t items = (int64_t)nwaves * ny / R;
         const int64_t blocks = std::min<int64_t>((items + 7) / 8, num_sms());
-        const size_t sm = sizeof(float2) * ((size_t)(kPipeThreads / 32) * R * L::SCR_STRIDE_ROW + 2 * N + kExpTab) +
+        const size_t sm = sizeof(float2) * ((size_t)(kPipeThreads / 32) * R * L::SCR_STRIDE_ROW + N + kExpTab) +
                           sizeof(float) * (size_t)(kPipeThreads / 32) * 2 * R * N;
         smem_attr(k_row_p<N>, sm);
         k_row_p<N><<<(unsigned)blocks, kPipeThreads, sm, st>>>(a, nwaves);
@@ -697,7 +869,7 @@ static bool col_pipe(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
         using L = FftLayout<N>;
         const int64_t items = (int64_t)nwaves * (nx / L::TC);
         const int64_t blocks = std::min<int64_t>(items, num_sms());
-        const size_t sm = sizeof(float2) * ((size_t)L::TC * L::SCR_STRIDE_COL + 2 * N + (size_t)N * L::TC);
+        const size_t sm = sizeof(float2) * ((size_t)L::TC * L::SCR_STRIDE_COL + N + (size_t)N * L::TC);
         smem_attr(k_col_p<N>, sm);
         k_col_p<N><<<(unsigned)blocks, kPipeThreads, sm, st>>>(a, nwaves);
         return true;
@@ -746,10 +918,13 @@ void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st
         smem_attr(k_row<N, ROW_INV_T_FWD_X>, sm);
         k_row<N, ROW_INV_T_FWD_X><<<grid, block, sm, st>>>(a);
         break;
-    case ROW_INV_TT_FWD:
-        smem_attr(k_row<N, ROW_INV_TT_FWD>, sm);
-        k_row<N, ROW_INV_TT_FWD><<<grid, block, sm, st>>>(a);
-        break;
+    case ROW_INV_TT_FWD: {
+        auto kern = a.l2_mode == L2_WAVES_RESIDENT ? k_row_tt<N, L2_WAVES_RESIDENT>
+                                                   : (a.l2_mode == L2_SHARED_T ? k_row_tt<N, L2_SHARED_T>
+                                                                               : k_row_tt<N, L2_DEFAULT>);
+        smem_attr(kern, sm);
+        kern<<<grid, block, sm, st>>>(a);
+    } break;
     case ROW_TT_FWD:
         smem_attr(k_row<N, ROW_TT_FWD>, sm);
         k_row<N, ROW_TT_FWD><<<grid, block, sm, st>>>(a);
@@ -764,6 +939,9 @@ void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st
     using L = FftLayout<N>;
     if (op == COL_STEP && a.variant == PASS_PIPELINED && !(a.flags & PF_FILTER_AUX) && ((uintptr_t)a.prop & 15) == 0 &&
         col_pipe<N>(a, nwaves, nx, st))
+        return;
+    // the hot column step reads its tile through the tensor memory accelerator
+    if (op == COL_STEP && a.variant == PASS_CLASSIC && !(a.flags & PF_FILTER_AUX) && col_step_tma<N>(a, nwaves, nx, st))
         return;
     dim3 grid((unsigned)(nwaves * (nx / L::TC))), block(L::COL_THREADS);
     size_t sm = L::COL_SMEM;

@@ -220,6 +220,14 @@ ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
  * generates each slice's potential just before its transmission, transmission_function.cuh:82-134). */
 ms_status ms_set_potential_overlap(ms_ctx* ctx, int enable);
 
+/* Host-side fault injection for tests of the failure paths (no reference counterpart).
+ * MS_INJECT_WAIT_TIMEOUT makes the column passes of the TEM/ED/CBED loop wait for a shared-memory
+ * tile that is never completed: the bounded device-side wait runs out after about a millisecond,
+ * the kernel records it and returns, and the call fails with MS_ERR_TIMEOUT; the context stays
+ * usable.  MS_INJECT_NONE (0) switches injection off. */
+enum { MS_INJECT_NONE = 0, MS_INJECT_WAIT_TIMEOUT = 1 };
+ms_status ms_set_fault_injection(ms_ctx* ctx, int what);
+
 /* Per-kernel timing (no reference counterpart: the reference has no tracing).  While enabled,
  * every fused pass and potential launch is bracketed by CUDA events on the context stream;
  * ms_profile_get returns the launches and summed device time of one kernel class
