@@ -154,11 +154,17 @@ def cpu_baseline(config: str, p_full, budget_s: float = 20.0):
     orc.set_threads(threads)
     if config == "cbed":
         p, at = wl.cbed_si(cells=(16, 16, 60), nconf=1)
-        sample = "1 of the 8 phonon configurations (240 slices) of the 1024^2 Si CBED workload"
+        sample = ("1 of the 8 phonon configurations (240 slices) of the 1024^2 Si CBED workload, FP64 host "
+                  "multislice; fp32 = the same with the wave, FFTs, transmission and propagator in FP32")
         t = time.perf_counter()
         orc.simulate_cbed(p, at)
         dt = time.perf_counter() - t
         units = 240
+        t = time.perf_counter()
+        orc.simulate_cbed_f32(p, at)
+        dt32 = time.perf_counter() - t
+        return {"value": units / dt, "unit": "probe*slice/s", "cores": threads, "kind": "port", "sample": sample,
+                "seconds": dt, "fp32": {"value": units / dt32, "unit": "probe*slice/s", "seconds": dt32}}
     elif config == "stem":
         p, at = wl.stem_sto(nconf=1, scan=(2, 1))
         sample = "2 probes x 50 slices of the 1024^2 SrTiO3 STEM workload"
@@ -218,6 +224,18 @@ def extras(ctx):
                     "run_STEM_general_simu form, potential regenerated per probe and slice (2 probes)",
         "unit": "probe*slice/s", "batched": batched, "autotuned_batch": B, "plain": b1, "ratio": batched / b1,
         "general_scan": general, "ratio_vs_general_scan": batched / general}
+
+    # the batched STEM workload at its full size, one call: 64x64 probe positions x 10 phonon
+    # configurations x 50 slices (2.05 M probe-slices), against the plain per-probe rate above
+    p, at = wl.stem_sto()
+    units_c3 = p.scan_nx * p.scan_ny * p.pn_nconf * 50
+    sim.executionSTEM(p, at)
+    full = units_c3 / (ctx.last_device_ms / 1e3)
+    out["stem_batched_vs_plain"].update({
+        "full_workload": "STEM ADF SrTiO3[001] 16x16x25 cells, 1024^2, 50 slices, 200 kV, 22 mrad, 64x64 probes on a "
+                         "0.2 A step x 10 phonon configurations, one call (device time)",
+        "full_batched": full, "full_autotuned_batch": ctx.last_probe_batch, "full_ms": ctx.last_device_ms,
+        "full_ratio": full / b1})
 
     # adjoint vs forward (SrTiO3 10x10x40 cells, 512^2, 80 slices, 16 probes, checkpoints every 8)
     p, at, xy = wl.adjoint_sto(n_probe=16)

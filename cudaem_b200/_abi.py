@@ -29,7 +29,7 @@ MS_TSI_TEMPORAL_SPATIAL, MS_TSI_TEMPORAL, MS_TSI_SPATIAL, MS_TSI_COHERENT = 1, 2
 MS_RECORD_INTENSITY, MS_RECORD_WAVE = 0, 1
 MS_EXEC_BATCHED, MS_EXEC_PLAIN, MS_EXEC_GENERAL = 0, 1, 2
 MS_BORDER_MIN, MS_BORDER_MAX, MS_BORDER_MIDDLE = 0, 1, 2
-MS_INJECT_NONE, MS_INJECT_WAIT_TIMEOUT = 0, 1
+MS_INJECT_NONE, MS_INJECT_WAIT_TIMEOUT, MS_INJECT_ALLOC_FAIL = 0, 1, 2
 
 
 class ms_lens(C.Structure):

@@ -181,7 +181,7 @@ ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
 
 ms_status ms_set_fault_injection(ms_ctx* c, int what)
 {
-    if (!c || (what != MS_INJECT_NONE && what != MS_INJECT_WAIT_TIMEOUT)) return MS_ERR_INVALID_ARG;
+    if (!c || what < MS_INJECT_NONE || what > MS_INJECT_ALLOC_FAIL) return MS_ERR_INVALID_ARG;
     c->inject = what;
     return MS_OK;
 }

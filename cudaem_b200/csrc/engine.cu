@@ -56,7 +56,7 @@ void* ms_ctx::buf(const std::string& name, size_t bytes)
     }
     size_t want = std::max<size_t>(bytes, 256);
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = inject == MS_INJECT_ALLOC_FAIL ? cudaErrorMemoryAllocation : cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         cudaGetLastError();
         throw msb::MsError(MS_ERR_OUT_OF_MEMORY,
@@ -1627,7 +1627,7 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
     const int nseg = (S + k - 1) / k;
     // probes per batch: adjoint wave, forward wave, one segment of transmitted waves and the
     // checkpoints must fit the memory budget
-    const size_t per_wave = (size_t)N * 8 * (2 + 2 * (size_t)k + (size_t)(nseg - 1));
+    const size_t per_wave = (size_t)N * 8 * (2 + 2 * (size_t)k + (size_t)(nseg - 1)) + (size_t)N * 4;
     int B = p.probe_batch > 0 ? p.probe_batch : 256;
     B = (int)std::max<size_t>(1, std::min<size_t>((size_t)B, free_budget(c) / per_wave));
     B = std::min(B, np);
@@ -1638,6 +1638,7 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
     float2* xseg = (float2*)c->buf("adj_xseg", sizeof(float2) * N * B * k * 2);
     float2* ckpt = nseg > 1 ? (float2*)c->buf("adj_ckpt", sizeof(float2) * N * B * (nseg - 1)) : nullptr;
     float* gV = on_dev ? dV : (float*)c->buf("adj_dV", sizeof(float) * slot);
+    float* gVw = (float*)c->buf("adj_dVw", sizeof(float) * N * B);   // per-wave planes of one slice
     double* partial = (double*)c->buf("det_part", sizeof(double) * B * nblk * ndet);
     double* Iw = (double*)c->buf("det_I", sizeof(double) * B * ndet);
     double* resid = (double*)c->buf("adj_resid", sizeof(double) * B * ndet);
@@ -1732,9 +1733,10 @@ void sim_stem_backward(ms_ctx* c, const ms_params& p, const float* V, int S, int
                 pa.slice = i;
                 pa.flags = 0;
                 pa.xs = xbuf(seg) + (int64_t)(i - c0) * wstride;
-                pa.dV = gV + (int64_t)i * N;
+                pa.dV = gVw;
                 pa.tw = s.tw_x;
                 run_row(c, p.nx, ROW_ADJ, pa, nb, p.ny, st);
+                launch_sum_waves(gVw, nb, N, gV + (int64_t)i * N, st);
                 pa.tw = s.tw_y;
                 if (i > 0) {
                     pa.slice = i - 1;

@@ -62,8 +62,9 @@ struct ElemTable {
     ElemCoef4 c[MS_NR];   // cubic coefficients of node i, packed for one 16-byte load
     float rmax, rmax2;
     float l0, inv_dl;   // log2(R2[0]) and nodes per log2 unit, for the direct index guess
+    float l0s;          // -l0 * inv_dl: the index guess is floor(log2(r2) * inv_dl + l0s)
     int Z;
-    int pad[3];
+    int pad[2];
 };
 void build_elem_table(const ms_params& p, int Z, ElemTable* t);
 // Projected potential V_z(R) and dV_z/dR^2 of an element, before tapering (FP64).

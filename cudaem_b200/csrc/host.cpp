@@ -266,6 +266,7 @@ void build_elem_table(const ms_params& p, int Z, ElemTable* t)
     t->rmax2 = (float)(rmx * rmx);
     t->l0 = (float)std::log2(R2[0]);
     t->inv_dl = (float)((MS_NR - 1) / std::log2(R2[MS_NR - 1] / R2[0]));
+    t->l0s = -t->l0 * t->inv_dl;
     t->Z = Z;
 }
 

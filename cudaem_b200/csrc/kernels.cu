@@ -174,6 +174,23 @@ void launch_resid(const double* I, const float* target, int n, double* resid, do
     check_launch("loss residuals");
 }
 
+// Adds the per-wave planes of one slice's dL/dV into the gradient, wave by wave in a fixed order.
+__global__ void k_sum_waves(const float* in, int nwaves, int64_t N, float* out)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    float s = out[p];
+    for (int b = 0; b < nwaves; b++) s += in[(int64_t)b * N + p];
+    out[p] = s;
+}
+
+void launch_sum_waves(const float* in, int nwaves, int64_t N, float* out, cudaStream_t st)
+{
+    k_sum_waves<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(in, nwaves, N, out);
+    count_launch();
+    check_launch("dL/dV sum over waves");
+}
+
 // Sums the lens-phase gradient partials of every wave in a fixed order into acc[0..1].
 __global__ void k_chi_finalize(const double* part, int n, double* acc)
 {
@@ -241,8 +258,8 @@ __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
     // log2(r2) on the node scale; a guess off by one (r2 within the log2 rounding, ~1e-6, of a
     // node) evaluates the neighbouring cubic a hair outside its interval, which the Hermite
     // spline's continuity of value and slope makes equal to 1e-12.
-    float lr = __log2f(fmaxf(r2, 1e-30f));
-    int i = __float2int_rd((lr - T.l0) * T.inv_dl);
+    // log2(r2) for r2 = 0 is -inf, which the floor conversion and the clamp turn into node 0
+    int i = __float2int_rd(fmaf(__log2f(r2), T.inv_dl, T.l0s));
     i = min(max(i, 0), MS_NR - 2);
     float d = r2 - T.R2[i];
     const ElemCoef4 c = T.c[i];
@@ -253,8 +270,7 @@ __device__ __forceinline__ float spline_eval(const ElemTable& T, float r2)
 // the same with the cubic coefficients read from a per-pair table (fine slicing)
 __device__ __forceinline__ float spline_eval_c(const ElemTable& T, const float4* __restrict__ coef, float r2)
 {
-    float lr = __log2f(fmaxf(r2, 1e-30f));
-    int i = __float2int_rd((lr - T.l0) * T.inv_dl);
+    int i = __float2int_rd(fmaf(__log2f(r2), T.inv_dl, T.l0s));
     i = min(max(i, 0), MS_NR - 2);
     float d = r2 - T.R2[i];
     const float4 c = __ldg(coef + i);

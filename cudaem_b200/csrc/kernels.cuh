@@ -96,7 +96,7 @@ struct PassArgs {
     float filt_g2in, filt_g2out;
     // adjoint
     float2* xs;               // [B][ny][nx] transmitted real-space waves t_s psi_s of one slice
-    float* dV;                // [ny][nx] dL/dV of one slice, accumulated over waves
+    float* dV;                // [B][ny][nx] each wave's dL/dV contribution of one slice
     const double* resid;      // [B][ndet] 4 (I - target) per wave and detector
     const float* det_thr;     // [2][ndet] inner, outer g^2 thresholds
     int ndet;
@@ -214,6 +214,8 @@ void launch_fill_c(float2* p, int64_t n, float2 v, cudaStream_t st);
 // adjoint helpers
 void launch_resid(const double* I, const float* target, int n, double* resid, double* sq, cudaStream_t st);
 void launch_chi_finalize(const double* part, int nwaves, int nparts, double* acc, cudaStream_t st);
+// out[p] += sum over b = 0..nwaves-1, in that order, of in[b N + p]
+void launch_sum_waves(const float* in, int nwaves, int64_t N, float* out, cudaStream_t st);
 int col_tiles(int N, int nx);
 
 int64_t kernel_launches();     // running count of this library's launches

@@ -98,12 +98,14 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
         for (int pass = (OP == ROW_T_FWD || OP == ROW_TT_FWD) ? 1 : 0; pass < 2; pass++) {
             if (pass == 0) conj_all(v);
             else if (OP == ROW_ADJ) {
+                // each wave's dL/dV contribution goes to its own plane of a.dV ([B][ny][nx]); the planes
+                // are summed in a fixed order afterwards, so the gradient is reproducible bit for bit
                 const float2* xr = a.xs + row_off;
-                float* gr = a.dV + (size_t)r * N;
+                float* gr = a.dV + row_off;
 #pragma unroll
                 for (int j = 0; j < E; j++) {
                     const float2 x = __ldg(xr + g + G * j);
-                    atomicAdd(gr + g + G * j, x.x * v[j].y - x.y * v[j].x);
+                    gr[g + G * j] = x.x * v[j].y - x.y * v[j].x;
                     v[j] = cmulc(v[j], expi_tab(__ldg(vr + g + G * j), etab));
                 }
             } else if (!beyond) {

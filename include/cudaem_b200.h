@@ -224,8 +224,10 @@ ms_status ms_set_potential_overlap(ms_ctx* ctx, int enable);
  * MS_INJECT_WAIT_TIMEOUT makes the column passes of the TEM/ED/CBED loop wait for a shared-memory
  * tile that is never completed: the bounded device-side wait runs out after about a millisecond,
  * the kernel records it and returns, and the call fails with MS_ERR_TIMEOUT; the context stays
- * usable.  MS_INJECT_NONE (0) switches injection off. */
-enum { MS_INJECT_NONE = 0, MS_INJECT_WAIT_TIMEOUT = 1 };
+ * usable.  MS_INJECT_ALLOC_FAIL makes every device allocation the context would make fail, as a
+ * cudaMalloc that ran out of memory: the call fails with MS_ERR_OUT_OF_MEMORY and the context
+ * stays usable.  MS_INJECT_NONE (0) switches injection off. */
+enum { MS_INJECT_NONE = 0, MS_INJECT_WAIT_TIMEOUT = 1, MS_INJECT_ALLOC_FAIL = 2 };
 ms_status ms_set_fault_injection(ms_ctx* ctx, int what);
 
 /* Per-kernel timing (no reference counterpart: the reference has no tracing).  While enabled,
@@ -317,8 +319,8 @@ ms_status ms_stem_forward_potential_noalloc(void* cuda_stream, const ms_params* 
  * lens (C10 includes z_init; C30 is Cs).  The waves are checkpointed every p->ckpt_interval
  * slices and each segment's transmitted waves are recomputed from its checkpoint.  V and
  * dL_dV are device pointers when V_on_device is 1, host pointers otherwise; probe_xy and
- * target ([n_probe][n_det]) are host memory.  dL/dV is summed over probes with atomic adds,
- * so its last bits may differ between runs.  No reference counterpart: the reference has no
+ * target ([n_probe][n_det]) are host memory.  dL/dV is summed over probes in a fixed order, so
+ * repeated calls give the same bits.  No reference counterpart: the reference has no
  * differentiable path. */
 ms_status ms_stem_backward(ms_ctx* ctx, const ms_params* p, const float* V, int n_slices, int V_on_device,
                            double z_init, const double* probe_xy, int n_probe, const float* target,

@@ -1706,6 +1706,144 @@ int or_stem_loss_fd(const ms_params* p, const float* V, int n_slices, double z_i
     return 0;
 }
 
+/* wave_modulation / wave_modulation_batch (wave_function.cuh:60-87) on caller phases and incident
+   waves: for every slice but the last, transmit then FFT, then P then inverse FFT; the last
+   slice transmits and FFTs, leaving the exit waves in reciprocal space.  V [S][ny][nx] float,
+   psi0 and out [B][ny][nx] complex (interleaved). */
+int or_slice_loop(const ms_params* p, const float* V, int S, int B, const double* psi0, double* out)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    long N = s.N;
+    cplx* P = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+    double* Vd = (double*)malloc(sizeof(double) * (size_t)N * S);
+    or_propagator(p, &s, P);
+    for (long k = 0; k < N * S; k++) Vd[k] = (double)V[k];
+    cplx* w = (cplx*)out;
+    memcpy(w, psi0, sizeof(cplx) * (size_t)N * B);
+    for (int b = 0; b < B; b++) or_multislice(&s, w + (size_t)b * N, Vd, S, P, p, NULL, NULL, NULL, NULL);
+    free(Vd);
+    free(P);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP32 host multislice (CPU baseline only): the CBED loop of or_tem_like with */
+/* the wave, its FFTs, the transmission and the propagator in single          */
+/* precision; potentials, probe and pattern sums as in the FP64 path.         */
+/* ------------------------------------------------------------------------ */
+typedef float complex fcplx;
+
+static void or_fft1f(fcplx* a, int n, int sign, const fcplx* tw)
+{
+    for (int i = 1, j = 0; i < n; i++) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            fcplx t = a[i];
+            a[i] = a[j];
+            a[j] = t;
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        int step = n / len;
+        for (int i = 0; i < n; i += len) {
+            for (int k = 0; k < len / 2; k++) {
+                fcplx w = tw[k * step];
+                if (sign > 0) w = conjf(w);
+                fcplx u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+        }
+    }
+}
+
+static fcplx* or_twiddlesf(int n)
+{
+    fcplx* t = (fcplx*)malloc(sizeof(fcplx) * (size_t)(n / 2 > 0 ? n / 2 : 1));
+    for (int k = 0; k < n / 2; k++) {
+        double a = -2.0 * OR_PI * (double)k / (double)n;
+        t[k] = (float)cos(a) + I * (float)sin(a);
+    }
+    return t;
+}
+
+static void or_fft2cf(fcplx* d, int nx, int ny, int sign, const fcplx* twx, const fcplx* twy)
+{
+    int nth = or_get_threads();
+#pragma omp parallel for num_threads(nth) schedule(static)
+    for (int r = 0; r < ny; r++) or_fft1f(d + (size_t)r * nx, nx, sign, twx);
+#pragma omp parallel num_threads(nth)
+    {
+        fcplx* col = (fcplx*)malloc(sizeof(fcplx) * (size_t)ny);
+#pragma omp for schedule(static)
+        for (int c = 0; c < nx; c++) {
+            for (int r = 0; r < ny; r++) col[r] = d[(size_t)r * nx + c];
+            or_fft1f(col, ny, sign, twy);
+            for (int r = 0; r < ny; r++) d[(size_t)r * nx + c] = col[r];
+        }
+        free(col);
+    }
+}
+
+int or_simulate_cbed_f32(const ms_params* p, const ms_atoms* a, double* img)
+{
+    or_sim s;
+    or_sim_init(p, &s);
+    int c0, c1;
+    double w;
+    or_confs(p, &c0, &c1, &w);
+    long N = s.N;
+    memset(img, 0, sizeof(double) * (size_t)N);
+    cplx* wd = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+    cplx* Pd = (cplx*)malloc(sizeof(cplx) * (size_t)N);
+    fcplx* wv = (fcplx*)malloc(sizeof(fcplx) * (size_t)N);
+    fcplx* P = (fcplx*)malloc(sizeof(fcplx) * (size_t)N);
+    double* V = (double*)malloc(sizeof(double) * (size_t)N);
+    fcplx* twx = or_twiddlesf(s.nx);
+    fcplx* twy = or_twiddlesf(s.ny);
+    or_propagator(p, &s, Pd);
+    for (long k = 0; k < N; k++) P[k] = (float)creal(Pd[k]) + I * (float)cimag(Pd[k]);
+    or_elems* es = (or_elems*)calloc(1, sizeof(or_elems));
+    ms_params q = *p;
+    if (q.iw_type < 0) q.iw_type = MS_IW_CONVERGENT;
+    for (int c = c0; c <= c1; c++) {
+        or_spec sp;
+        or_spec_build(p, a, c, &sp);
+        or_incident(&q, &s, p->iw_x, p->iw_y, sp.z_init, wd);
+        for (long k = 0; k < N; k++) wv[k] = (float)creal(wd[k]) + I * (float)cimag(wd[k]);
+        for (int i = 0; i < sp.ns; i++) {
+            or_slice_potential(p, a, &s, &sp, es, i, V);
+            for (long k = 0; k < N; k++) {
+                float v = (float)V[k];
+                wv[k] *= cosf(v) + I * sinf(v);
+            }
+            or_fft2cf(wv, s.nx, s.ny, -1, twx, twy);
+            if (i < sp.ns - 1) {
+                for (long k = 0; k < N; k++) wv[k] *= P[k];
+                or_fft2cf(wv, s.nx, s.ny, +1, twx, twy);
+            }
+        }
+        for (long k = 0; k < N; k++) {
+            double re = crealf(wv[k]), im = cimagf(wv[k]);
+            img[k] += w * (re * re + im * im);
+        }
+        or_spec_free(&sp);
+    }
+    or_fftshift(img, s.nx, s.ny);
+    free(es);
+    free(twx);
+    free(twy);
+    free(V);
+    free(P);
+    free(wv);
+    free(Pd);
+    free(wd);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* operator-level entry points, checked against the reference's own kernels  */
 /* (oracle/ref_shim) on the same inputs                                      */

@@ -56,9 +56,16 @@ int or_simulate_stem(const ms_params* p, const ms_atoms* a, double* stem);
 int or_simulate_thickness(const ms_params* p, const ms_atoms* a, double* frames, int64_t cap,
                           int* n_frames);
 
+/* CBED with the wave, FFTs, transmission and propagator in FP32 (the CPU baseline's FP32 figure) */
+int or_simulate_cbed_f32(const ms_params* p, const ms_atoms* a, double* img);
+
 /* HRTEM defocus series: images at objective C10 + df[i], [nd][ny][nx] */
 int or_simulate_tem_series(const ms_params* p, const ms_atoms* a, int nd, const double* df, double* img, double* re,
                            double* im);
+
+/* the slice loop alone (wave_modulation) on caller phases V[S][ny][nx] and incident waves psi0
+   [B][ny][nx] (interleaved complex): the exit waves in reciprocal space into out */
+int or_slice_loop(const ms_params* p, const float* V, int S, int B, const double* psi0, double* out);
 
 /* raw STEM forward / adjoint on caller phase arrays V[n_slices][ny][nx] */
 int or_stem_forward_potential(const ms_params* p, const float* V, int n_slices, double z_init,

@@ -33,6 +33,23 @@ def build() -> str:
 _REF = None
 
 
+REF_LOOP_PATH = os.path.join(HERE, "_ref", "libref_loop.so")
+_REF_LOOP = None
+
+
+def ref_loop_lib():
+    """The reference's composed slice loop through its cuFFT callbacks (oracle/_ref/libref_loop.so),
+    or None when it was not built."""
+    global _REF_LOOP
+    if _REF_LOOP is None and os.path.exists(REF_LOOP_PATH):
+        L = C.CDLL(REF_LOOP_PATH)
+        P, f, i = C.POINTER, C.c_float, C.c_int
+        L.ref_slice_loop.restype = i
+        L.ref_slice_loop.argtypes = [i, i, P(f), i, P(f), P(f), P(f)]
+        _REF_LOOP = L
+    return _REF_LOOP
+
+
 def ref_lib():
     """The reference-kernel shim (oracle/_ref/libref_kernels.so), or None when it was not built."""
     global _REF
@@ -77,6 +94,8 @@ def lib() -> C.CDLL:
             "or_simulate_tem": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), P(d), P(d)]),
             "or_simulate_cbed": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), P(d), P(d)]),
             "or_simulate_tem_series": (i, [P(abi.ms_params), P(abi.ms_atoms), i, P(d), P(d), P(d), P(d)]),
+            "or_simulate_cbed_f32": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d)]),
+            "or_slice_loop": (i, [P(abi.ms_params), P(f), i, i, P(d), P(d)]),
             "or_simulate_stem": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d)]),
             "or_simulate_thickness": (i, [P(abi.ms_params), P(abi.ms_atoms), P(d), C.c_int64, P(i)]),
             "or_stem_forward_potential": (i, [P(abi.ms_params), P(f), i, d, P(d), i, P(d)]),
@@ -211,6 +230,35 @@ def simulate_tem_series(params, atoms, defocus):
         return re, im
     img = np.empty(n)
     lib().or_simulate_tem_series(C.byref(p), C.byref(a), df.size, _d(df), _d(img), None, None)
+    return img
+
+
+def slice_loop(params, V, psi0):
+    """The slice loop alone on phases V [S][ny][nx] and incident waves psi0 [B][ny][nx] (complex):
+    the exit waves in reciprocal space, [B][ny][nx] complex128."""
+    V = np.ascontiguousarray(V, np.float32)
+    psi0 = np.ascontiguousarray(psi0, np.complex128).reshape(-1, params.ny, params.nx)
+    out = np.empty_like(psi0)
+    p = params.c()
+    lib().or_slice_loop(C.byref(p), _f(V), V.shape[0], psi0.shape[0], _d(psi0.view(np.float64)),
+                        _d(out.view(np.float64)))
+    return out
+
+
+def incident(params, px, py, z_init):
+    """The incident wave (plane wave, or the convergent probe at (px, py) with defocus shift
+    z_init), in real space, as complex128 [ny][nx]."""
+    W = np.empty((params.ny, params.nx), np.complex128)
+    p = params.c()
+    lib().or_op_probe(C.byref(p), px, py, z_init, _d(W.view(np.float64)))
+    return np.fft.ifft2(W) * W.size
+
+
+def simulate_cbed_f32(params, atoms):
+    """CBED intensity with the multislice loop in FP32 (the CPU baseline's single-precision path)."""
+    img = np.empty((params.ny, params.nx))
+    p, a = params.c(), atoms.c()
+    lib().or_simulate_cbed_f32(C.byref(p), C.byref(a), _d(img))
     return img
 
 

@@ -66,3 +66,22 @@ def test_a_planted_error_is_caught(gold):
     out = np.empty(2 * p.nx * p.ny)
     orc.lib().or_op_propagator(C.byref(p.c()), out.ctypes.data_as(C.POINTER(C.c_double)))
     assert rel_l2(_c(out), _c(gold["propagator__out"])) > TOL
+
+
+def test_oracle_slice_loop_against_reference_loop_golden():
+    """The oracle's composed slice loop against the reference's own loop (its cuFFT plans and load
+    callbacks, run on a B200 by tests/golden/make_golden.py loop), sampled at fixed pixels."""
+    import ref_loop_cases as rl
+    from oracle import oracle as orc
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_loop.npz")
+    g = np.load(path)
+    for name in rl.CASES:
+        p, V, psi0 = rl.build(name)
+        want = orc.slice_loop(p, V, psi0)
+        idx = g[f"{name}__idx"]
+        assert np.array_equal(idx, rl.sample_index(want.shape[1] * want.shape[2]))
+        got = g[f"{name}__out"].astype(np.complex128)
+        w = want.reshape(want.shape[0], -1)[:, idx]
+        assert rel_l2(got, w) < 1e-5, name
+        # the whole exit waves' norms, as the reference computed them
+        assert np.allclose(g[f"{name}__norm"], np.linalg.norm(want.reshape(want.shape[0], -1), axis=1), rtol=1e-5)

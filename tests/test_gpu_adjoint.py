@@ -63,10 +63,21 @@ def test_checkpoint_interval_does_not_change_gradients(ctx):
         p.ckpt_interval = k
         got = ctx.stem_backward(p, V, z0, xy, T)
         assert abs(got[0] - ref[0]) <= 1e-12 * abs(ref[0])
-        # atomic accumulation over probes may reorder the last bits of dL/dV
-        assert rel_l2(got[1], ref[1]) < 1e-6
+        # the segments are recomputed with the same kernels on the same inputs and dL/dV is summed
+        # over probes in a fixed order, so the gradient does not depend on the checkpoint spacing
+        assert np.array_equal(got[1], ref[1])
         assert abs(got[2] - ref[2]) <= 1e-9 * abs(ref[2])
         assert abs(got[3] - ref[3]) <= 1e-9 * abs(ref[3])
+
+
+def test_backward_is_reproducible(ctx):
+    """Two calls on the same inputs give the same bits (dL/dV is summed over probes in a fixed
+    order, not with atomic adds)."""
+    p, V, xy, z0, T = _problem(256, 6, 9, seed=31, ckpt=2, batch=4)
+    a = ctx.stem_backward(p, V, z0, xy, T)
+    b = ctx.stem_backward(p, V, z0, xy, T)
+    assert a[0] == b[0] and a[2] == b[2] and a[3] == b[3]
+    assert np.array_equal(a[1], b[1])
 
 
 def test_backward_against_finite_differences(ctx):

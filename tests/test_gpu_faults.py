@@ -39,3 +39,35 @@ def test_fault_injection_rejects_unknown_codes():
     with cb.Context(0) as ctx:
         with pytest.raises(cb.MsError):
             ctx.set_fault_injection(7)
+
+
+def test_allocation_failure_and_context_recovers():
+    """Every device allocation of the call fails (as cudaMalloc out of memory): the call reports
+    MS_ERR_OUT_OF_MEMORY; the same context then allocates and runs normally."""
+    p, at = cases.cbed_small(n=128, nconf=2)
+    with cb.Context(0) as ctx:
+        sim = cb.MulSimulator(ctx=ctx)
+        ctx.set_fault_injection(abi.MS_INJECT_ALLOC_FAIL)
+        with pytest.raises(cb.MsError) as e:
+            sim.executionCBED(p, at)
+        assert e.value.status == abi.MS_ERR_OUT_OF_MEMORY
+        ctx.set_fault_injection(abi.MS_INJECT_NONE)
+        out = sim.executionCBED(p, at)
+        assert rel_l2(out.image_intensity, orc.simulate_cbed(p, at)) < 1e-5
+
+
+def test_allocation_failure_mid_stem_batches():
+    """A STEM call fails part-way on a grown buffer (a larger scan needs larger batch buffers than
+    the call before it): MS_ERR_OUT_OF_MEMORY, and the context then completes the larger scan."""
+    small, at = cases.stem_small(n=128, scan=(2, 1), nconf=1, batch=0)
+    large, _ = cases.stem_small(n=128, scan=(6, 5), nconf=1, batch=0)
+    with cb.Context(0) as ctx:
+        sim = cb.MulSimulator(ctx=ctx)
+        sim.executionSTEM(small, at)          # buffers sized for two probes
+        ctx.set_fault_injection(abi.MS_INJECT_ALLOC_FAIL)
+        with pytest.raises(cb.MsError) as e:
+            sim.executionSTEM(large, at)
+        assert e.value.status == abi.MS_ERR_OUT_OF_MEMORY
+        ctx.set_fault_injection(abi.MS_INJECT_NONE)
+        out = sim.executionSTEM(large, at)
+        assert rel_l2(out.stem_intensity, orc.simulate_stem(large, at)) < 1e-5

@@ -244,3 +244,9 @@ def test_tilted_plane_wave_vacuum():
     peak = np.unravel_index(np.argmax(img), img.shape)
     assert peak == (p.ny // 2, p.nx // 2 + m)
     assert img[peak] / img.sum() > 1 - 1e-9
+
+
+def test_fp32_host_multislice_tracks_fp64():
+    """The FP32 host multislice (the CPU baseline's single-precision figure) against the FP64 oracle."""
+    p, at = cases.cbed_small(nconf=2)
+    assert rel_l2(orc.simulate_cbed_f32(p, at), orc.simulate_cbed(p, at)) < 1e-4
