@@ -50,8 +50,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-vs-plain, adjoint and uneven-batch measurements")
-    ap.add_argument("--pass-kernels", type=int, default=0, choices=[0, 1],
-                    help="slice-pass kernel form: 0 classic (default), 1 persistent pipelined")
+    ap.add_argument("--pass-kernels", type=int, default=0, choices=[0, 1, 2],
+                    help="slice-pass kernel form: 0 classic (default), 1 persistent pipelined, "
+                         "2 persistent slice engine (every slice of a batch in one launch)")
     ap.add_argument("--potential-overlap", type=int, default=0, choices=[0, 1],
                     help="potentials: 0 all before the slice loop (default), 1 in chunks beside the slice passes")
     ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
@@ -419,7 +420,8 @@ def run_ours(args):
     ctx.profile_reset()
     step(co)
     torch.cuda.synchronize()
-    prof = {k: ctx.profile(k) for k in ("row", "col", "potential", "probe")}
+    prof = {k: ctx.profile(k) for k in ("row", "col", "potential", "probe", "engine")}
+    prof = {k: v for k, v in prof.items() if v[0] > 0}
     ctx.set_profiling(False)
     dom = max(prof, key=lambda k: prof[k][1])
     n_l, tot_ms = prof[dom]
@@ -430,6 +432,9 @@ def run_ours(args):
         # (row pass) the potential slice 4 N shared by S waves
         per_wave = 16 * N + (4 * N / S_share if dom == "row" else 0)
         algo = per_wave * waves
+    elif dom == "engine":
+        # one launch = every slice of the batch: a row and a column pass per wave and slice
+        algo = units * (32 * N + 4 * N / S_share)
     else:
         algo = 4 * N * (p.pn_nconf if args.config == "cbed" else 1)
     avg_s = tot_ms / max(1, n_l) / 1e3

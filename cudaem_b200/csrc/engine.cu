@@ -704,6 +704,73 @@ int l2_mode_for_waves(int nwaves, int64_t N)
     return (double)nwaves * (double)N * sizeof(float2) <= 72.0 * 1024 * 1024 ? L2_WAVES_RESIDENT : L2_DEFAULT;
 }
 
+// The whole slice loop of a wave batch in one persistent launch (slice_engine.cuh), from slice
+// `slice0` to each wave's last.  ns[w] is wave w's slice count; the items of slice s cover the
+// waves up to the last one with more than s slices (waves inside that prefix whose slices are
+// done skip their items).  engine_plan uploads the item table and clears the counters on the
+// stream; the launch that follows it (engine_launch, possibly captured in a graph) consumes them.
+EngineArgs engine_plan(ms_ctx* c, const std::vector<int>& ns, int slice0, int N, cudaStream_t st,
+                       unsigned long long* done_ns, const std::string& tag = std::string())
+{
+    const int nw = (int)ns.size();
+    int S_end = 0;
+    for (int v : ns) S_end = std::max(S_end, v);
+    const int S = std::max(0, S_end - slice0);
+    // row blocks / column tiles per work item: as many as keep the items of one slice phase at
+    // least four times the resident blocks (fewer, larger items mean fewer dependency checks and
+    // completion counts per slice)
+    int sub = 1;
+    const int64_t resident = 2LL * num_sms();
+    while (sub < 8 && (int64_t)nw * (N / engine_rows(N)) / (2 * sub) >= 4 * resident) sub *= 2;
+    const int RB = N / engine_rows(N) / sub, CT = N / engine_cols(N) / sub;
+    std::vector<int> start(2 * (size_t)S + 1);
+    int t = 0;
+    for (int j = 0; j < S; j++) {
+        int nact = nw;
+        while (nact > 0 && ns[nact - 1] <= slice0 + j) nact--;
+        start[2 * j] = t;
+        t += nact * RB;
+        start[2 * j + 1] = t;
+        t += nact * CT;
+    }
+    start[2 * (size_t)S] = t;
+    EngineArgs e;
+    std::memset(&e, 0, sizeof(e));
+    e.state = (EngineState*)c->buf("eng_state" + tag, sizeof(EngineState));
+    int* dstart = (int*)c->buf("eng_start" + tag, sizeof(int) * start.size());
+    unsigned* cnt = (unsigned*)c->buf("eng_cnt" + tag, sizeof(unsigned) * 2 * nw);
+    CK(cudaMemsetAsync(e.state, 0, sizeof(EngineState), st));
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * 2 * nw, st));
+    // pageable source: the copy has read the table when the call returns
+    CK(cudaMemcpyAsync(dstart, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, st));
+    e.phase_start = dstart;
+    e.n_items = t;
+    e.S_max = S;
+    e.slice0 = slice0;
+    e.sub = sub;
+    e.rows_done = cnt;
+    e.cols_done = cnt + nw;
+    e.done_ns = done_ns;
+    return e;
+}
+
+// Whether the engine can run a batch: square grids (one layout serves rows and columns) and the
+// plain slice step (no stored inputs, filters or vacuum continuation).
+bool engine_fits(const ms_ctx* c, int nx, int ny, int flags)
+{
+    return c->pass_variant == PASS_ENGINE && nx == ny &&
+           !(flags & (PF_STORE_X | PF_FILTER_AUX | PF_VACUUM_BEYOND | PF_PROP_ALWAYS | PF_TILT_INCIDENT));
+}
+
+void engine_launch(const PassArgs& pa, const EngineArgs& e, int N, int nwaves, cudaStream_t st)
+{
+    if (e.n_items <= 0) return;
+    EngineArgs ee = e;
+    ee.wait_cycles = pa.wait_cycles;
+    if (!launch_slice_engine(N, pa.tt ? ROW_INV_TT_FWD : ROW_INV_T_FWD, pa, ee, nwaves, st))
+        throw MsError(MS_ERR_INTERNAL, "the slice engine could not be launched (wave alignment or tensor map)");
+}
+
 // Device time and launches of one call; the context's wait-error word is cleared at the start and
 // read at the end (a kernel whose bounded wait ran out has set it).
 struct Timer {
@@ -720,7 +787,8 @@ struct Timer {
         CK(cudaEventSynchronize(c->ev1));
         int e = 0;
         CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (e) throw MsError(MS_ERR_TIMEOUT, "a device-side wait for a shared-memory tile ran out");
+        if (e & 1) throw MsError(MS_ERR_TIMEOUT, "a device-side wait for a shared-memory tile ran out");
+        if (e) throw MsError(MS_ERR_TIMEOUT, "a device-side wait for another block's slice work ran out");
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
         c->last_ms = ms;
@@ -853,7 +921,11 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         }
         const int S_max = *std::max_element(g.ns.begin(), g.ns.end());
         const bool plane = iw == MS_IW_PLANE || iw == MS_IW_PLANE_TILTED;
-        for (int sl = 0; sl < S_max; sl++) {
+        // with the persistent engine, a plane wave's first slice (no inverse row transform, the
+        // tilt) runs as separate passes and the engine takes the slices after it
+        const bool eng = engine_fits(c, p.nx, p.ny, pa.flags);
+        const int sl_end = eng ? (plane ? std::min(1, S_max) : 0) : S_max;
+        for (int sl = 0; sl < sl_end; sl++) {
             pc.wait(c, sl);
             pa.slice = sl;
             pa.tw = s.tw_x;
@@ -864,6 +936,14 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
             PassArgs pc = pa;
             if (c->inject == MS_INJECT_WAIT_TIMEOUT) pc.flags |= PF_TEST_WAIT;
             run_col(c, p.ny, COL_STEP, pc, nw, p.nx, st);
+        }
+        if (eng) {
+            for (int sl = sl_end; sl < S_max; sl++) pc.wait(c, sl);
+            PassArgs pe = pa;
+            pe.tw = s.tw_x;
+            if (c->inject == MS_INJECT_WAIT_TIMEOUT) pe.flags |= PF_TEST_WAIT;
+            const EngineArgs e = engine_plan(c, g.ns, sl_end, p.nx, st, nullptr);
+            timed(c, "engine", [&] { engine_launch(pe, e, p.nx, nw, st); });
         }
         const int illum = p.illumination_model ? p.illumination_model : MS_ILLUM_COHERENT;
         const int tsi = p.temporal_spatial_incoh ? p.temporal_spatial_incoh : MS_TSI_TEMPORAL_SPATIAL;
@@ -1338,11 +1418,18 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
             pa.l2_mode = plain ? L2_DEFAULT : L2_SHARED_T;   // one transmission slice serves the whole batch
             pa.tt = sT;
             if (!plain) {
+                const bool eng = engine_fits(c, p.nx, p.ny, pa.flags);
+                EngineArgs e;
+                if (eng) e = engine_plan(c, std::vector<int>((size_t)nb, S), 0, p.nx, st, nullptr);
                 auto body = [&] {
                     PassArgs q = pa;
                     q.tw = s.tw_y;
                     run_col(c, p.ny, COL_PROBE_INV, q, nb, p.nx, st);
-                    for (int sl = 0; sl < S; sl++) {
+                    if (eng) {
+                        q.tw = s.tw_x;
+                        timed(c, "engine", [&] { engine_launch(q, e, p.nx, nb, st); });
+                    }
+                    for (int sl = 0; sl < (eng ? 0 : S); sl++) {
                         q.slice = sl;
                         q.tw = s.tw_x;
                         run_row(c, p.nx, ROW_INV_T_FWD, q, nb, p.ny, st);
@@ -1823,6 +1910,11 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
         }
     } evfree{&done};
     for (int i = 0; i < n; i++) CK(cudaEventCreate(&done[i]));
+    // instances that run in the persistent engine report the device clock at which their waves
+    // were done, against this stamp of the call's start
+    unsigned long long* t0_ns = (unsigned long long*)c->buf("many_t0", sizeof(unsigned long long));
+    launch_stamp(t0_ns, st);
+    std::vector<unsigned long long> inst_done_ns((size_t)n, 0ull);
 
     // per instance: physics, propagator table, potential store
     struct Inst {
@@ -1927,6 +2019,8 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             double* acc = nullptr;
             cudaStream_t s = nullptr;
             int S_max = 0;
+            size_t done_off = 0;        // first entry of the group's waves in the completion clocks
+            bool engine = false;        // the group runs in the persistent slice engine
         };
         std::vector<Group> groups;
         for (int i = r0; i < r1; i++) {
@@ -1942,10 +2036,16 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
         // tables every group reads, made before the groups fork off the context stream
         if (!c->exptab) make_setup(c, ps[r0]);
         const float2* ex = (const float2*)c->exptab;
+        size_t nwaves_all = 0;
         for (Group& G : groups) {
             twiddles(c, G.nx);
             twiddles(c, G.ny);
+            G.done_off = nwaves_all;
+            for (int i : G.inst) nwaves_all += in[i].waves.size();
+            G.engine = engine_fits(c, G.nx, G.ny, 0);
         }
+        unsigned long long* dns = (unsigned long long*)c->buf("many_done_ns", sizeof(unsigned long long) * nwaves_all);
+        CK(cudaMemsetAsync(dns, 0, sizeof(unsigned long long) * nwaves_all, st));
         cudaEvent_t fork = chunk_event(c, 0);
         CK(cudaEventRecord(fork, st));
         for (size_t gi = 0; gi < groups.size(); gi++) {
@@ -1979,13 +2079,37 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
                 launch_col(G.ny, COL_PROBE_INV, pa, I.nconf, G.nx, G.s);
             }
         }
+        // groups in the engine: every slice of every instance in one launch, then the patterns
+        for (size_t gi = 0; gi < groups.size(); gi++) {
+            Group& G = groups[gi];
+            if (!G.engine) continue;
+            std::vector<int> ns;
+            for (const WaveInfo& w : G.waves) ns.push_back(w.n_slices);
+            const EngineArgs e = engine_plan(c, ns, 0, G.nx, G.s, dns + G.done_off, "_many" + std::to_string(gi));
+            PassArgs pa;
+            std::memset(&pa, 0, sizeof(pa));
+            pa.psi = G.psi;
+            pa.waves = G.dwv;
+            pa.exptab = ex;
+            pa.grid = in[G.inst.front()].gd;
+            pa.err = c->d_err;
+            pa.tw = twiddles(c, G.nx);
+            engine_launch(pa, e, G.nx, (int)G.waves.size(), G.s);
+            const int64_t N = (int64_t)G.nx * G.ny;
+            for (size_t kk = 0; kk < G.inst.size(); kk++) {
+                const int i = G.inst[kk];
+                launch_acc_abs2(G.psi + (int64_t)G.off[kk] * N, in[i].nconf, G.dwv + G.off[kk], N, G.acc, 1, G.s);
+                launch_emit(G.acc, G.nx, G.ny, 1, in[i].out, G.s);
+                CK(cudaEventRecord(done[i], G.s));
+            }
+        }
         int S_all = 0;
         for (Group& G : groups) S_all = std::max(S_all, G.S_max);
         std::vector<size_t> next((size_t)groups.size(), 0);   // next instance (in S order) to finish, per group
         for (int sl = 0; sl < S_all; sl++) {
             for (size_t gi = 0; gi < groups.size(); gi++) {
                 Group& G = groups[gi];
-                if (sl >= G.S_max) continue;
+                if (G.engine || sl >= G.S_max) continue;
                 // active waves: instances with slices left form a prefix
                 size_t ki = 0;
                 while (ki < G.inst.size() && in[G.inst[ki]].S_max > sl) ki++;
@@ -2022,6 +2146,16 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
         for (int i = r0; i < r1; i++) copy_out(c, outs[i].image_intensity, in[i].out, (int64_t)ps[i].nx * ps[i].ny,
                                                outs[i].on_device);
         CK(cudaStreamSynchronize(st));
+        if (lat) {
+            std::vector<unsigned long long> h(nwaves_all);
+            CK(cudaMemcpy(h.data(), dns, sizeof(unsigned long long) * nwaves_all, cudaMemcpyDeviceToHost));
+            for (const Group& G : groups) {
+                if (!G.engine) continue;
+                for (size_t kk = 0; kk < G.inst.size(); kk++)
+                    for (int k = 0; k < in[G.inst[kk]].nconf; k++)
+                        inst_done_ns[G.inst[kk]] = std::max(inst_done_ns[G.inst[kk]], h[G.done_off + G.off[kk] + k]);
+            }
+        }
         // buffers of instances that outgrew the arena are this call's alone
         for (int i = r0; i < r1; i++) {
             for (const char* nm : {"many_sV_", "many_prop_", "many_out_"}) {
@@ -2047,6 +2181,12 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, c->ev0, done[i]));
             lat[i] = ms;
+            if (inst_done_ns[i]) {
+                // engine instances: the device clock when the instance's last wave was done
+                unsigned long long t0 = 0;
+                CK(cudaMemcpy(&t0, t0_ns, sizeof(t0), cudaMemcpyDeviceToHost));
+                if (inst_done_ns[i] > t0) lat[i] = (double)(inst_done_ns[i] - t0) * 1e-6;
+            }
         }
     }
 }

@@ -145,6 +145,58 @@ void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream
     check_launch("column pass");
 }
 
+__global__ void k_stamp(unsigned long long* dst)
+{
+    unsigned long long ns;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns));
+    *dst = ns;
+}
+
+void launch_stamp(unsigned long long* dst, cudaStream_t st)
+{
+    k_stamp<<<1, 1, 0, st>>>(dst);
+    count_launch();
+    check_launch("stamp");
+}
+
+bool launch_slice_engine(int N, int rowop, const PassArgs& a, const EngineArgs& e, int nwaves, cudaStream_t st)
+{
+    bool ok = false;
+    switch (N) {
+    case 128: ok = engine_dispatch<128>(rowop, a, e, nwaves, st); break;
+    case 256: ok = engine_dispatch<256>(rowop, a, e, nwaves, st); break;
+    case 512: ok = engine_dispatch<512>(rowop, a, e, nwaves, st); break;
+    case 1024: ok = engine_dispatch<1024>(rowop, a, e, nwaves, st); break;
+    case 2048: ok = engine_dispatch<2048>(rowop, a, e, nwaves, st); break;
+    default: throw MsError(MS_ERR_UNSUPPORTED, "unsupported transform length");
+    }
+    if (ok) {
+        count_launch();
+        check_launch("slice engine");
+    }
+    return ok;
+}
+
+// the thread layout of the engine (slice_engine.cuh): threads = max(row, column threads)
+template <int N>
+static int engine_rows_n()
+{
+    using L = FftLayout<N>;
+    return (L::ROW_THREADS > L::COL_THREADS ? L::ROW_THREADS : L::COL_THREADS) / L::G;
+}
+int engine_rows(int N)
+{
+    switch (N) {
+    case 128: return engine_rows_n<128>();
+    case 256: return engine_rows_n<256>();
+    case 512: return engine_rows_n<512>();
+    case 1024: return engine_rows_n<1024>();
+    case 2048: return engine_rows_n<2048>();
+    }
+    throw MsError(MS_ERR_UNSUPPORTED, "unsupported transform length");
+}
+int engine_cols(int N) { return col_tiles(N, N) > 0 ? N / col_tiles(N, N) : 0; }
+
 int col_tiles(int N, int nx)
 {
     switch (N) {

@@ -114,10 +114,28 @@ enum L2Mode {
     L2_SHARED_T = 2         // one transmission slice serves every wave: transmission evict-last, waves evict-first
 };
 
+// The persistent slice engine's bookkeeping (slice_engine.cuh).  The ticket, the per-wave item
+// counters and the completion times live in device memory and start at zero.
+struct EngineState {
+    unsigned ticket;
+    unsigned pad[31];
+};
+struct EngineArgs {
+    EngineState* state;
+    const int* phase_start;        // [2 S_max + 1]: first ticket of (slice slice0 + j, phase), k = 2 j + (column)
+    int n_items, S_max;            // S_max: slices in the launch (slice0 .. slice0 + S_max - 1)
+    int slice0;                    // first slice of the launch (earlier slices are done)
+    int sub;                       // row blocks / column tiles per work item (a power of two <= 8)
+    unsigned* rows_done;           // [nwaves] row items done (all slices)
+    unsigned* cols_done;           // [nwaves] column items done
+    unsigned long long* done_ns;   // [nwaves] device clock when the wave's last slice was done (may be null)
+    long long wait_cycles;         // limit of a dependency wait (0: about one second)
+};
+
 // Kernel form of ROW_INV_T_FWD and COL_STEP: the classic one-block-per-tile kernels (two
 // resident blocks per SM, the default: measured faster on B200 at 1024^2) or the persistent
 // pipelined kernels (grids of 128..1024 points).  Both compute the same operations.
-enum PassVariant { PASS_CLASSIC = 0, PASS_PIPELINED = 1 };
+enum PassVariant { PASS_CLASSIC = 0, PASS_PIPELINED = 1, PASS_ENGINE = 2 };
 
 // Spatial cells of the atom binning: a ncx x ncy grid of square cells of side 1/inv_cell.
 struct CellGrid {
@@ -159,11 +177,21 @@ struct ElemCoefDev;
 // slice passes of one transform length (passes_<N>.cu)
 template <int N>
 void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st);
+// the persistent slice engine over nwaves square N x N waves (rowop ROW_INV_TT_FWD or
+// ROW_INV_T_FWD); false when it cannot run here (the tensor map could not be made)
+template <int N>
+bool engine_dispatch(int rowop, const PassArgs& a, const EngineArgs& e, int nwaves, cudaStream_t st);
 template <int N>
 void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
 
 // launchers (kernels.cu); all asynchronous on `st`
 void launch_row(int N, int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st);
+void launch_stamp(unsigned long long* dst, cudaStream_t st);   // *dst = the device clock (ns)
+bool launch_slice_engine(int N, int rowop, const PassArgs& a, const EngineArgs& e, int nwaves, cudaStream_t st);
+// rows of one engine row item and columns of one column item at transform length N
+int engine_rows(int N);
+int num_sms();   // streaming multiprocessors of the current device
+int engine_cols(int N);
 void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
 size_t row_smem(int N);
 size_t col_smem(int N);

@@ -943,7 +943,7 @@ void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st
         col_pipe<N>(a, nwaves, nx, st))
         return;
     // the hot column step reads its tile through the tensor memory accelerator
-    if (op == COL_STEP && a.variant == PASS_CLASSIC && !(a.flags & PF_FILTER_AUX) && col_step_tma<N>(a, nwaves, nx, st))
+    if (op == COL_STEP && a.variant != PASS_PIPELINED && !(a.flags & PF_FILTER_AUX) && col_step_tma<N>(a, nwaves, nx, st))
         return;
     dim3 grid((unsigned)(nwaves * (nx / L::TC))), block(L::COL_THREADS);
     size_t sm = L::COL_SMEM;
@@ -978,6 +978,32 @@ void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st
         break;
     default: throw MsError(MS_ERR_INTERNAL, "unknown column pass");
     }
+}
+
+}  // namespace msb
+
+#include "slice_engine.cuh"
+
+namespace msb {
+
+template <int N>
+bool engine_dispatch(int rowop, const PassArgs& a, const EngineArgs& e, int nwaves, cudaStream_t st)
+{
+    using L = FftLayout<N>;
+    using EL = EngineLayout<N>;
+    if (((uintptr_t)a.psi & 15) != 0 || e.n_items <= 0) return false;
+    CUtensorMap map;
+    if (!encode_wave_tile_map(&map, a.psi, N, (int64_t)nwaves * N, 2 * L::TC, N < 256 ? N : 256)) return false;
+    auto kern = rowop != ROW_INV_TT_FWD          ? k_slice_engine<N, ROW_INV_T_FWD, L2_DEFAULT>
+                : a.l2_mode == L2_WAVES_RESIDENT ? k_slice_engine<N, ROW_INV_TT_FWD, L2_WAVES_RESIDENT>
+                : a.l2_mode == L2_SHARED_T       ? k_slice_engine<N, ROW_INV_TT_FWD, L2_SHARED_T>
+                                                 : k_slice_engine<N, ROW_INV_TT_FWD, L2_DEFAULT>;
+    smem_attr(kern, EL::SMEM);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, EL::THREADS, EL::SMEM);
+    const int64_t blocks = std::min<int64_t>(e.n_items, (int64_t)num_sms() * std::max(1, per_sm));
+    kern<<<(unsigned)blocks, EL::THREADS, EL::SMEM, st>>>(a, e, map);
+    return true;
 }
 
 }  // namespace msb

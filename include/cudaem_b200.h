@@ -207,9 +207,12 @@ ms_status ms_set_graphs(ms_ctx* ctx, int enable);
 /* Kernel form of the hot slice passes: 0 (default) the classic kernels, one block per tile
  * of rows or columns with two blocks resident per SM; 1 the persistent pipelined kernels
  * (one block per SM walking the work items, the next item's wave prefetched while the
- * current one is transformed) for grids of 128..1024 points per axis.  Both compute the same
- * operations (results agree to float rounding); the choice only changes speed.  No
- * reference counterpart (the reference's passes are cuFFT plans). */
+ * current one is transformed) for grids of 128..1024 points per axis; 2 the persistent slice
+ * engine: on square grids, every slice of a CBED / TEM / STEM batch or of an uneven batch's
+ * grid group runs in one launch whose blocks take row and column work items in slice order
+ * and wait (bounded) for each wave's earlier items through per-wave slice counters.  All
+ * forms compute the same operations (results agree to float rounding); the choice only
+ * changes speed.  No reference counterpart (the reference's passes are cuFFT plans). */
 ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
 /* Order of the projected-potential work in the TEM, ED, CBED and thickness simulations:
  * 0 (default) every slice's potential before the slice loop, on the context stream; 1 the
