@@ -184,10 +184,12 @@ def cpu_baseline(config: str, p_full, budget_s: float = 20.0):
             "seconds": dt}
 
 
-def extras(ctx):
-    """The metric's other two legs and the uneven batch, each device-timed through the C ABI:
-    batched STEM against the one-probe-per-launch path, the adjoint against a forward pass,
-    and the 64-instance uneven batch with its completion-latency percentiles."""
+def extras(ctx, pass_kernels: int = 0):
+    """The metric's other two legs, the uneven batch and the HRTEM image, each device-timed through
+    the C ABI: batched STEM against the one-probe-per-launch path, the adjoint against a forward
+    pass, the 64-instance uneven batch with its completion-latency percentiles and its roofline,
+    and one 512^2 HRTEM image (a single wave).  The STEM batch and the uneven batch are also timed
+    in the persistent slice engine (pass-kernel form 2)."""
     import ctypes as C
 
     import torch
@@ -225,6 +227,10 @@ def extras(ctx):
                     "run_STEM_general_simu form, potential regenerated per probe and slice (2 probes)",
         "unit": "probe*slice/s", "batched": batched, "autotuned_batch": B, "plain": b1, "ratio": batched / b1,
         "general_scan": general, "ratio_vs_general_scan": batched / general}
+    ctx.set_pass_kernels(2)
+    eng, _ = stem_rate(p, at)
+    ctx.set_pass_kernels(pass_kernels)
+    out["stem_batched_vs_plain"].update({"batched_engine": eng, "ratio_engine": eng / b1})
 
     # the batched STEM workload at its full size, one call: 64x64 probe positions x 10 phonon
     # configurations x 50 slices (2.05 M probe-slices), against the plain per-probe rate above
@@ -279,15 +285,60 @@ def extras(ctx):
 
     # uneven batch: 64 CBED instances, 256^2..2048^2, 10-200 slices, 80-300 kV, 10-30 mrad
     jobs = wl.uneven_mix(64)
-    sim.executionMany(jobs)
-    outs, lat = sim.executionMany(jobs)
-    units = sum(o.n_slices * max(1, p.pn_nconf) for (p, _), o in zip(jobs, outs))
-    ms = ctx.last_device_ms
-    out["uneven_batch"] = {"workload": "64 CBED instances drawn from seed 42: grids 256^2..2048^2, 10-200 slices "
-                                       "of SrTiO3 or Si, 80-300 kV, 10-30 mrad, one phonon configuration each",
-                           "unit": "probe*slice/s", "value": units / (ms / 1e3), "ms": ms, "probe_slices": units,
-                           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
-                                          "p99": float(np.percentile(lat, 99)), "max": float(lat.max())}}
+    peak, peak_kind = peaks()
+
+    def uneven(variant):
+        ctx.set_pass_kernels(variant)
+        sim.executionMany(jobs)
+        best = None
+        for _ in range(2):
+            outs, lat = sim.executionMany(jobs)
+            if best is None or ctx.last_device_ms < best[0]:
+                best = (ctx.last_device_ms, outs, lat)
+        ctx.set_pass_kernels(pass_kernels)
+        ms, outs, lat = best
+        units = sum(o.n_slices * max(1, p.pn_nconf) for (p, _), o in zip(jobs, outs))
+        # algorithmic bytes: per probe-slice 16 N (wave read + write) + 4 N (the instance's sigma V)
+        algo = sum(20.0 * p.nx * p.ny * o.n_slices * max(1, p.pn_nconf) for (p, _), o in zip(jobs, outs))
+        gbs = algo / (ms / 1e3) / 1e9
+        return {"unit": "probe*slice/s", "value": units / (ms / 1e3), "ms": ms, "probe_slices": units,
+                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                               "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+                "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                             "peak_source": peak_kind, "algorithmic_bytes": algo,
+                             "note": "whole call (specimens, potentials, slice passes, patterns) against the "
+                                     "sum of every instance's 20 N bytes per probe-slice"}}
+
+    out["uneven_batch"] = dict(workload="64 CBED instances drawn from seed 42: grids 256^2..2048^2, 10-200 slices "
+                                        "of SrTiO3 or Si, 80-300 kV, 10-30 mrad, one phonon configuration each",
+                               **uneven(0))
+    out["uneven_batch"]["engine"] = uneven(2)
+    out["uneven_batch"]["engine"]["note"] = ("persistent slice engine (one launch per grid group); latency = the "
+                                             "device clock at which an instance's last wave was done")
+
+    # HRTEM: one 512^2 plane wave, 40 slices, CTF image (a single wave: latency bound)
+    p, at = wl.hrtem_sto()
+    sim.executionTEM(p, at)
+    t = []
+    for _ in range(5):
+        sim.executionTEM(p, at)
+        t.append(ctx.last_device_ms)
+    ms = min(t)
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    sim.executionTEM(p, at)
+    prof = {k: round(ctx.profile(k)[1], 4) for k in ("row", "col", "potential")}
+    nl = {k: ctx.profile(k)[0] for k in ("row", "col")}
+    ctx.set_profiling(False)
+    host = time.perf_counter()
+    for _ in range(5):
+        sim.executionTEM(p, at)
+    e2e_ms = (time.perf_counter() - host) * 1e3 / 5
+    out["hrtem"] = {"workload": "HRTEM SrTiO3[001] 10x10x20 cells, 512^2, 40 slices, 200 kV plane wave, coherent "
+                                "CTF image, one configuration", "unit": "probe*slice/s",
+                    "value": 40 / (ms / 1e3), "ms": ms, "e2e": {"value": 40 / (e2e_ms / 1e3), "ms": e2e_ms},
+                    "kernel_ms": prof, "launches": nl,
+                    "slice_us": {k: 1e3 * prof[k] / max(1, nl[k]) for k in ("row", "col")}}
     return out
 
 
@@ -454,7 +505,7 @@ def run_ours(args):
                          "kernel_share": {k: v[1] for k, v in prof.items()}},
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_extras:
-        line.update(extras(ctx))
+        line.update(extras(ctx, args.pass_kernels))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.config, p)
     if rank == 0:

@@ -377,6 +377,8 @@ __global__ void __launch_bounds__(kPotThreads, 8) k_potential(PotArgs a)
     unsigned* candp = reinterpret_cast<unsigned*>(cand + kPotThreads);   // fine slicing: pair index
     __shared__ int wsum[kPotThreads / 32];
     __shared__ int total_s;
+    // per warp: the candidates whose disc reaches the warp's 16 x 16 pixel block (indices into cand)
+    __shared__ unsigned short whit[kPotThreads / 32][kPotThreads];
     __shared__ unsigned r_beg[kPotMaxRanges], r_pre[kPotMaxRanges + 1];
     __shared__ int r_img[kPotMaxRanges];
     __shared__ int n_ranges;
@@ -532,20 +534,35 @@ __global__ void __launch_bounds__(kPotThreads, 8) k_potential(PotArgs a)
             }
             __syncthreads();
             const int total = total_s;
-            for (int q = 0; q < total; q++) {
+            // The warp's own list, one candidate per lane: an atom whose disc misses the warp's 16 x 16
+            // pixel block is dropped here (its spline evaluations would all be masked off, yet a
+            // divergent warp still issues them), so the loop below runs over hits only.
+            int nh = 0;
+            for (int base = 0; base < total; base += 32) {
+                const int q = base + lane;
+                bool hit = false;
+                if (q < total) {
+                    const float4 cd = cand[q];
+                    const int bits = __float_as_int(cd.w);
+                    const float rmax2 = el[bits & 0xFF].rmax2;
+                    const int ox = ((bits >> 8) & 15) - 4, oy = ((bits >> 12) & 15) - 4;
+                    const float xs = cd.x + (float)ox * a.lx, ys = cd.y + (float)oy * a.ly;
+                    const float dxr = fmaxf(0.f, fmaxf(WX0 - xs, xs - WX1));
+                    const float dyr = fmaxf(0.f, fmaxf(WY0 - ys, ys - WY1));
+                    hit = dxr * dxr + dyr * dyr < rmax2 * 1.0002f + 1e-4f;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (hit) whit[wid][nh + __popc(m & ((1u << lane) - 1u))] = (unsigned short)q;
+                nh += __popc(m);
+            }
+            __syncwarp();
+            for (int h = 0; h < nh; h++) {
+                const int q = whit[wid][h];
                 const float4 cd = cand[q];
                 const int bits = __float_as_int(cd.w);
                 const ElemTable& T = el[bits & 0xFF];
                 const float rmax2 = T.rmax2;
                 const int ox = ((bits >> 8) & 15) - 4, oy = ((bits >> 12) & 15) - 4;
-                // warp-uniform skip: the atom's disc misses this warp's 16 x 16 pixel block (its
-                // spline evaluations would all be masked off, yet a divergent warp still issues them)
-                {
-                    const float xs = cd.x + (float)ox * a.lx, ys = cd.y + (float)oy * a.ly;
-                    const float dxr = fmaxf(0.f, fmaxf(WX0 - xs, xs - WX1));
-                    const float dyr = fmaxf(0.f, fmaxf(WY0 - ys, ys - WY1));
-                    if (dxr * dxr + dyr * dyr >= rmax2 * 1.0002f + 1e-4f) continue;
-                }
                 // distance to the image (ox, oy) of the atom: pixel index shifted by -ox*nx, and
                 // i*dx - x formed with dx split in two floats, so the offset is accurate to its own
                 // rounding (the pixel coordinate i*dx alone would carry ~1e-6 A of error)
