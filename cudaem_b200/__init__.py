@@ -263,8 +263,21 @@ class Context:
         self.check(lib().ms_set_graphs(self.handle, 1 if enable else 0))
 
     def set_pass_kernels(self, variant: int) -> None:
-        """0: classic one-block-per-tile slice passes (default); 1: persistent pipelined passes."""
+        """0: classic one-block-per-tile slice passes (default); 1: persistent pipelined passes;
+        2: the persistent slice engine (every slice of a batch in one launch)."""
         self.check(lib().ms_set_pass_kernels(self.handle, variant))
+
+    def set_tile_shape(self, shape: int) -> None:
+        """-1: autotuned per grid and batch (default); 0: wide tiles; 1: narrow tiles."""
+        self.check(lib().ms_set_tile_shape(self.handle, int(shape)))
+
+    @property
+    def last_tile_shape(self) -> int:
+        return lib().ms_last_tile_shape(self.handle)
+
+    def set_tune_cache(self, path: Optional[str]) -> None:
+        """JSON file keeping the autotuner's choices across contexts (None: in the context only)."""
+        self.check(lib().ms_set_tune_cache(self.handle, path.encode() if path else None))
 
     def set_fault_injection(self, what: int) -> None:
         """Host-side fault injection for failure-path tests (abi.MS_INJECT_*)."""

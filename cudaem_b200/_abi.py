@@ -154,6 +154,9 @@ PROTOTYPES = {
     "ms_last_probe_batch": (C.c_int, [C.c_void_p]),
     "ms_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_set_pass_kernels": (C.c_int, [C.c_void_p, C.c_int]),
+    "ms_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int]),
+    "ms_last_tile_shape": (C.c_int, [C.c_void_p]),
+    "ms_set_tune_cache": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ms_set_potential_overlap": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_simulate_many": (C.c_int, [C.c_void_p, C.c_int, _P(ms_params), _P(ms_atoms), _P(ms_output),
                                    _P(C.c_double)]),

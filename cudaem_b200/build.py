@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels.cu", "passes_128.cu", "passes_256.cu", "passes_512.cu", "passes_1024.cu", "passes_2048.cu",
               "engine.cu", "noalloc.cu"]
-CPP_SOURCES = ["host.cpp", "abi.cpp"]
+CPP_SOURCES = ["host.cpp", "abi.cpp", "tune.cpp"]
 
 
 def _host_cxx() -> str:

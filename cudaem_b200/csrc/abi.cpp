@@ -179,6 +179,31 @@ ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
     return MS_OK;
 }
 
+ms_status ms_set_tile_shape(ms_ctx* c, int shape)
+{
+    if (!c || shape < -1 || shape > 1) return MS_ERR_INVALID_ARG;
+    c->tile_shape = shape;
+    if (c->stream) {
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+    }
+    c->drop_graph();   // captured graphs hold the other kernels
+    return MS_OK;
+}
+
+int ms_last_tile_shape(const ms_ctx* c) { return c ? c->last_tile : 0; }
+
+ms_status ms_set_tune_cache(ms_ctx* c, const char* path)
+{
+    if (!c) return MS_ERR_INVALID_ARG;
+    c->tune_path = path ? path : "";
+    if (!c->tune_path.empty()) {
+        cudaSetDevice(c->device);
+        msb::tune_load(c);
+    }
+    return MS_OK;
+}
+
 ms_status ms_set_fault_injection(ms_ctx* c, int what)
 {
     if (!c || what < MS_INJECT_NONE || what > MS_INJECT_ALLOC_FAIL) return MS_ERR_INVALID_ARG;

@@ -44,6 +44,11 @@ struct ms_ctx {
     cudaStream_t pot_stream = nullptr;           // potential chunks computed beside the slice passes
     std::vector<cudaEvent_t> chunk_ev;           // completion of each potential chunk
     std::map<std::string, int> batch_choice;     // autotuned probe batch per grid and slice count
+    std::map<std::string, int> tile_choice;      // autotuned tile shape per grid and batch
+    int tile_shape = -1;                         // forced msb::TileShape, or -1: autotuned
+    int last_tile = 0;                           // tile shape of the last call's hot passes
+    std::string tune_path;                       // JSON file that keeps the autotuner's choices ("": none)
+    std::string device_tag;                      // device name and SM count, the prefix of every tuning key
     void drop_graph();
 
     // per-kernel event timing
@@ -72,6 +77,11 @@ struct ms_ctx {
 
 namespace msb {
 void ctx_activate(ms_ctx* c);
+// The autotuner's JSON cache (tune.cpp): device_tag names the device in every key; tune_load
+// merges the file's entries for this device into the context, tune_save writes them back.
+std::string device_tag(ms_ctx* c);
+void tune_load(ms_ctx* c);
+void tune_save(ms_ctx* c);
 // A defocus series of HRTEM images: n offsets (Angstrom) added to the objective lens's C10.
 struct DefocusSeries {
     int n = 0;

@@ -704,6 +704,58 @@ int l2_mode_for_waves(int nwaves, int64_t N)
     return (double)nwaves * (double)N * sizeof(float2) <= 72.0 * 1024 * 1024 ? L2_WAVES_RESIDENT : L2_DEFAULT;
 }
 
+// Tile shape of the hot passes (row step on the transmission store, column step) for a batch of
+// nw waves on an nx x ny grid: forced by ms_set_tile_shape, else the faster of the wide and the
+// narrow tiles, timed on the call's own transmission store and wave descriptors with a scratch
+// wave (two slice steps per shape, after one untimed round).  The choice is kept per device, grid
+// and batch size in the context and in the JSON cache file when one is set.
+int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, cudaStream_t st)
+{
+    if (c->tile_shape >= 0) return c->tile_shape;
+    if (!pa.tt || pa.variant == PASS_PIPELINED) return TILE_WIDE;
+    char key[64];
+    std::snprintf(key, sizeof(key), "%d,%d,%d", nx, ny, nw);
+    auto it = c->tile_choice.find(key);
+    if (it != c->tile_choice.end()) return it->second;
+    if (c->profile) return TILE_WIDE;   // per-launch events would time the events
+    const int64_t N = (int64_t)nx * ny;
+    float2* scratch = (float2*)c->buf("tune_psi", sizeof(float2) * N * nw);
+    CK(cudaMemsetAsync(scratch, 0, sizeof(float2) * N * nw, st));
+    pa.psi = scratch;
+    pa.flags = 0;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best_ms = 0.f;
+    int best = TILE_WIDE;
+    for (int rep = 0; rep < 2; rep++) {   // the first round warms up both shapes
+        for (int shape : {TILE_WIDE, TILE_NARROW}) {
+            pa.tile = shape;
+            CK(cudaEventRecord(e0, st));
+            for (int sl = 0; sl < 2; sl++) {
+                pa.slice = sl;
+                pa.tw = twiddles(c, nx);
+                launch_row(nx, ROW_INV_T_FWD, pa, nw, ny, st);
+                pa.tw = twiddles(c, ny);
+                launch_col(ny, COL_STEP, pa, nw, nx, st);
+            }
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep == 1 && (shape == TILE_WIDE || ms < best_ms)) {
+                best_ms = ms;
+                best = shape;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tile_choice[key] = best;
+    tune_save(c);
+    return best;
+}
+
 // The whole slice loop of a wave batch in one persistent launch (slice_engine.cuh), from slice
 // `slice0` to each wave's last.  ns[w] is wave w's slice count; the items of slice s cover the
 // waves up to the last one with more than s slices (waves inside that prefix whose slices are
@@ -915,6 +967,8 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
         pa.l2_mode = l2_mode_for_waves(nw, N);
         pa.tt = sT;
+        pa.tile = choose_tile(c, pa, p.nx, p.ny, nw, st);
+        c->last_tile = pa.tile;
         if (iw == MS_IW_CONVERGENT) {
             pa.tw = s.tw_y;
             run_col(c, p.ny, COL_PROBE_INV, pa, nw, p.nx, st);
@@ -1153,6 +1207,7 @@ int autotune_batch(ms_ctx* c, const ms_params& p, const Setup& s, const PassArgs
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->batch_choice[key] = best;
+    tune_save(c);
     return best;
 }
 
@@ -1417,6 +1472,10 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
             PassArgs pa = pass_args(s, psi, dwv, nullptr, plain ? 0 : slot, cond);
             pa.l2_mode = plain ? L2_DEFAULT : L2_SHARED_T;   // one transmission slice serves the whole batch
             pa.tt = sT;
+            if (!plain) {
+                pa.tile = choose_tile(c, pa, p.nx, p.ny, nb, st);
+                c->last_tile = pa.tile;
+            }
             if (!plain) {
                 const bool eng = engine_fits(c, p.nx, p.ny, pa.flags);
                 EngineArgs e;

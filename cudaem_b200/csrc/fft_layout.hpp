@@ -61,17 +61,30 @@ struct FftCfg<2048> {
     static constexpr int G = 32, ROWS = 4, TC = 8;
 };
 
+// Narrow tiles for batches too small to fill the GPU (one 512^2 HRTEM wave has 32 wide row
+// blocks for 148 SMs): one warp of rows per row block, two columns per column block (the
+// narrowest tile a 16-byte tensor-memory-accelerator box allows).  The twiddles are then read
+// from global memory (L1) instead of being staged per block.
 template <int N>
-struct FftLayout {
+struct NarrowCfg {
+    static constexpr int G = FftCfg<N>::G;
+    static constexpr int ROWS = G >= 32 ? 1 : 32 / G;
+    static constexpr int TC = N < 256 ? 32 / G : 2;
+};
+
+template <int N, int ROWS_ = FftCfg<N>::ROWS, int TC_ = FftCfg<N>::TC>
+struct FftLayoutT {
     static constexpr int G = FftCfg<N>::G;
     static constexpr int E = N / G;
-    static constexpr int ROWS = FftCfg<N>::ROWS;
-    static constexpr int TC = FftCfg<N>::TC;
+    static constexpr int ROWS = ROWS_;
+    static constexpr int TC = TC_;
     static constexpr int ROW_THREADS = ROWS * G;
     static constexpr int COL_THREADS = TC * G;
-    static constexpr int COL_MINB = (N == 2048) ? 1 : 2;   // resident column blocks per SM (register cap)
+    static constexpr bool NARROW = ROWS_ != FftCfg<N>::ROWS || TC_ != FftCfg<N>::TC;
+    // resident blocks per SM that the register cap allows (__launch_bounds__)
+    static constexpr int COL_MINB = NARROW ? (N == 2048 ? 2 : 4) : ((N == 2048) ? 1 : 2);
     static constexpr bool COL_TW_GLOBAL = false;            // twiddles staged in shared memory
-    static constexpr int ROW_MINB = (N == 2048) ? 1 : 2;   // resident row blocks per SM (register cap)
+    static constexpr int ROW_MINB = NARROW ? (N == 2048 ? 4 : 8) : ((N == 2048) ? 1 : 2);
     // transpose scratch of one transform: E rows of G+1 slots, plus padding so that
     // consecutive transforms start on banks that keep a half-warp conflict-free
     static constexpr int SCR_BASE = E * (G + 1);
@@ -82,5 +95,12 @@ struct FftLayout {
     static constexpr size_t ROW_SMEM = sizeof(float2) * ((size_t)ROWS * SCR_STRIDE_ROW + N + 1024);
     static constexpr size_t COL_SMEM = sizeof(float2) * ((size_t)TC * SCR_STRIDE_COL + (COL_TW_GLOBAL ? 0 : N));
 };
+template <int N>
+using FftLayout = FftLayoutT<N>;
+template <int N>
+using NarrowLayout = FftLayoutT<N, NarrowCfg<N>::ROWS, NarrowCfg<N>::TC>;
+
+// Tile shape of the hot slice passes (PassArgs.tile)
+enum TileShape { TILE_WIDE = 0, TILE_NARROW = 1 };
 
 }  // namespace msb

@@ -102,6 +102,7 @@ struct PassArgs {
     int ndet;
     double* chi_part;         // [B][nx / TC][2] partial sums of g^2 q and g^4 q
     int variant;              // PassVariant of the row / column pass kernels (host side only)
+    int tile;                 // TileShape of the classic hot passes (host side only)
     int l2_mode;              // L2Mode: eviction priorities of the wave and transmission accesses
     int* err;                 // device word set to a nonzero code when a bounded device-side wait runs out
     long long wait_cycles;    // limit of such a wait in clock cycles (0: about one second)

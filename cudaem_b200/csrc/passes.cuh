@@ -155,10 +155,11 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
 // but the row's values (k_row's general form spills here).  Loads and stores carry the L2
 // eviction priorities of PassArgs.l2_mode, a template argument MODE (a policy chosen at run time
 // costs the registers that make the kernel spill).
-template <int N, int MODE>
-__global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_MINB) k_row_tt(PassArgs a)
+// L is the tile layout: FftLayout<N> (wide, the default) or NarrowLayout<N> (one warp of rows per
+// block, twiddles read from global memory).
+template <int N, int MODE, class L = FftLayout<N>>
+__global__ void __launch_bounds__(L::ROW_THREADS, L::ROW_MINB) k_row_tt(PassArgs a)
 {
-    using L = FftLayout<N>;
     constexpr int G = L::G, E = L::E;
     extern __shared__ float2 smem[];
     const int ny = a.grid.ny;
@@ -174,9 +175,15 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
 #pragma unroll
         for (int j = 0; j < E; j++) v[j] = src[G * j];
     }
-    float2* tw = smem + L::ROWS * L::SCR_STRIDE_ROW;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_set<N>(a)[i];
-    __syncthreads();
+    const float2* tw;
+    if constexpr (L::NARROW) {
+        tw = tw_set<N>(a);
+    } else {
+        float2* tws = smem + L::ROWS * L::SCR_STRIDE_ROW;
+        for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = tw_set<N>(a)[i];
+        __syncthreads();
+        tw = tws;
+    }
     float2* scr_base = smem + team * L::SCR_STRIDE_ROW;
     auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
     auto sync = []() { __syncwarp(); };
@@ -432,11 +439,10 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
 // the copy engine moves the tile in large requests and leaves the load/store unit free.  The wait
 // for the tile is bounded (PassArgs.wait_cycles): when it runs out the block records the failure
 // in PassArgs.err and returns.  The arithmetic is k_col's COL_STEP.
-template <int N>
-__global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_MINB)
+template <int N, class L = FftLayout<N>>
+__global__ void __launch_bounds__(L::COL_THREADS, L::COL_MINB)
     k_col_step_tma(PassArgs a, const __grid_constant__ CUtensorMap tmap)
 {
-    using L = FftLayout<N>;
     constexpr int G = L::G, E = L::E, TC = L::TC;
     constexpr int BOX = N < 256 ? N : 256;
     constexpr unsigned TILE_BYTES = (unsigned)(N * TC * sizeof(float2));
@@ -462,7 +468,9 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
 #pragma unroll
         for (int q = 0; q < N / BOX; q++) tma_load_2d(tile + q * BOX * TC, &tmap, 2 * col0, b * N + q * BOX, &bar);
     }
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = tw_set<N>(a)[i];
+    if constexpr (!L::NARROW)
+        for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = tw_set<N>(a)[i];
+    const float2* twp = L::NARROW ? tw_set<N>(a) : tws;
     __syncthreads();
     const long long limit = (a.flags & PF_TEST_WAIT) ? 2000000LL : (a.wait_cycles > 0 ? a.wait_cycles : kWaitCycles);
     const bool late = !mbar_wait_bounded(&bar, 0, limit);
@@ -480,7 +488,7 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
     const size_t cs = (size_t)G * nx;
 #pragma unroll 1
     for (int pass = 0; pass < 2; pass++) {
-        team_fft<N, G, -1>(v, g, tws, scr, sync);
+        team_fft<N, G, -1>(v, g, twp, scr, sync);
         if (pass == 1) {
             conj_all(v);
             break;
@@ -503,19 +511,18 @@ __global__ void __launch_bounds__(FftLayout<N>::COL_THREADS, FftLayout<N>::COL_M
     for (int j = 0; j < E; j++) st_l2hint(cp + j * cs, v[j], pol);
 }
 
-template <int N>
+template <int N, class L = FftLayout<N>>
 static bool col_step_tma(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
 {
     if constexpr (N < 256) {
         return false;
     } else {
-        using L = FftLayout<N>;
         if (((uintptr_t)a.psi & 15) != 0) return false;
         CUtensorMap map;
         if (!encode_wave_tile_map(&map, a.psi, nx, (int64_t)nwaves * N, 2 * L::TC, N < 256 ? N : 256)) return false;
         const size_t sm = L::COL_SMEM + 128;
-        smem_attr(k_col_step_tma<N>, sm);
-        k_col_step_tma<N><<<(unsigned)(nwaves * (nx / L::TC)), L::COL_THREADS, sm, st>>>(a, map);
+        smem_attr(k_col_step_tma<N, L>, sm);
+        k_col_step_tma<N, L><<<(unsigned)(nwaves * (nx / L::TC)), L::COL_THREADS, sm, st>>>(a, map);
         return true;
     }
 }
@@ -895,6 +902,17 @@ void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st
     if (op == ROW_INV_TT_FWD && a.variant == PASS_PIPELINED && ((uintptr_t)a.psi & 15) == 0 &&
         row_q<N>(a, nwaves, ny, st))
         return;
+    if (op == ROW_INV_TT_FWD && a.tile == TILE_NARROW) {
+        // one warp of rows per block; only the transpose scratch lives in shared memory
+        using NL = NarrowLayout<N>;
+        auto kern = a.l2_mode == L2_WAVES_RESIDENT ? k_row_tt<N, L2_WAVES_RESIDENT, NL>
+                    : a.l2_mode == L2_SHARED_T     ? k_row_tt<N, L2_SHARED_T, NL>
+                                                   : k_row_tt<N, L2_DEFAULT, NL>;
+        const size_t nsm = sizeof(float2) * (size_t)NL::ROWS * NL::SCR_STRIDE_ROW;
+        smem_attr(kern, nsm);
+        kern<<<(unsigned)(nwaves * (ny / NL::ROWS)), NL::ROW_THREADS, nsm, st>>>(a);
+        return;
+    }
     switch (op) {
     case ROW_T_FWD:
         smem_attr(k_row<N, ROW_T_FWD>, sm);
@@ -943,8 +961,10 @@ void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st
         col_pipe<N>(a, nwaves, nx, st))
         return;
     // the hot column step reads its tile through the tensor memory accelerator
-    if (op == COL_STEP && a.variant != PASS_PIPELINED && !(a.flags & PF_FILTER_AUX) && col_step_tma<N>(a, nwaves, nx, st))
-        return;
+    if (op == COL_STEP && a.variant != PASS_PIPELINED && !(a.flags & PF_FILTER_AUX)) {
+        if (a.tile == TILE_NARROW && col_step_tma<N, NarrowLayout<N>>(a, nwaves, nx, st)) return;
+        if (col_step_tma<N>(a, nwaves, nx, st)) return;
+    }
     dim3 grid((unsigned)(nwaves * (nx / L::TC))), block(L::COL_THREADS);
     size_t sm = L::COL_SMEM;
     switch (op) {

@@ -214,6 +214,20 @@ ms_status ms_set_graphs(ms_ctx* ctx, int enable);
  * forms compute the same operations (results agree to float rounding); the choice only
  * changes speed.  No reference counterpart (the reference's passes are cuFFT plans). */
 ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
+/* Tile shape of the classic hot passes (the row step on the transmission store and the column
+ * step): -1 (default) autotuned per grid and batch size, 0 wide tiles (blocks of 8..16 rows or
+ * 8..16 columns), 1 narrow tiles (one warp of rows, two columns per block) for batches too small
+ * to fill the GPU.  The autotuner times both shapes on the call's own data the first time a grid
+ * and batch size are seen.  Both shapes compute the same operations bit for bit.  No reference
+ * counterpart (the reference's FFTs are cuFFT plans). */
+ms_status ms_set_tile_shape(ms_ctx* ctx, int shape);
+/* Tile shape (0 wide, 1 narrow) of the last CBED / TEM / STEM call's hot passes. */
+int ms_last_tile_shape(const ms_ctx* ctx);
+/* JSON file that keeps the autotuner's choices (probe batch, tile shape) across contexts and
+ * processes, keyed by device, grid and batch size; entries already in the file are loaded now.
+ * NULL or "" keeps the choices in the context only (the default).  A missing or unreadable file
+ * starts empty; an unwritable one only loses the persistence. */
+ms_status ms_set_tune_cache(ms_ctx* ctx, const char* path);
 /* Order of the projected-potential work in the TEM, ED, CBED and thickness simulations:
  * 0 (default) every slice's potential before the slice loop, on the context stream; 1 the
  * potentials in 16-slice chunks, all but the first on a side stream while the slice passes of
