@@ -896,6 +896,66 @@ void ctx_activate(ms_ctx* c)
 // ---------------------------------------------------------------------------
 // HRTEM / ED (ED_HRTEM, single_simulator.cuh:11-126) and CBED (CBED_CBEI, :128-206)
 // ---------------------------------------------------------------------------
+namespace {
+// Launch arguments that a captured batch graph bakes in, as a byte string.
+std::string graph_key_of(const PassArgs& pa, int nb, int S, int nblk, int ndet, const void* partial,
+                         const void* Iw, const void* img, const void* thr, int npos)
+{
+    std::string k((const char*)&pa, sizeof(PassArgs));
+    const int ints[5] = {nb, S, nblk, ndet, npos};
+    const void* ptrs[4] = {partial, Iw, img, thr};
+    k.append((const char*)ints, sizeof(ints));
+    k.append((const char*)ptrs, sizeof(ptrs));
+    return k;
+}
+
+// Runs `body` (launches only) on the context stream through a cached CUDA graph: captured on
+// first use or when `key` changes, replayed otherwise.  Falls back to direct launches while
+// profiling (per-launch events), on the legacy default stream, or when the stream is already
+// being captured by the caller.
+template <class F>
+void run_graphed(ms_ctx* c, const std::string& key, F&& body)
+{
+    cudaStream_t st = c->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    bool ok = c->use_graphs && !c->profile && st != nullptr && st != cudaStreamLegacy &&
+              st != cudaStreamPerThread && cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
+              cs == cudaStreamCaptureStatusNone;
+    if (!ok) {
+        body();
+        return;
+    }
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) {
+        if (c->graphs.size() >= 4) c->drop_graph();   // full batches, the last partial batch, ...
+        const int64_t l0 = kernel_launches();
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            body();
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(st, &g));
+        cudaGraphExec_t ge = nullptr;
+        cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        ms_ctx::Graph gr;
+        gr.exec = ge;
+        gr.launches = kernel_launches() - l0;
+        add_kernel_launches(-gr.launches);   // captured, not run
+        it = c->graphs.emplace(key, gr).first;
+    }
+    CK(cudaGraphLaunch(it->second.exec, st));
+    add_kernel_launches(it->second.launches);
+}
+}  // namespace
+
 void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out, bool force_cbed,
                   const DefocusSeries* series)
 {
@@ -979,17 +1039,27 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         // tilt) runs as separate passes and the engine takes the slices after it
         const bool eng = engine_fits(c, p.nx, p.ny, pa.flags);
         const int sl_end = eng ? (plane ? std::min(1, S_max) : 0) : S_max;
-        for (int sl = 0; sl < sl_end; sl++) {
-            pc.wait(c, sl);
-            pa.slice = sl;
-            pa.tw = s.tw_x;
-            PassArgs pr = pa;
-            if (sl == 0 && iw == MS_IW_PLANE_TILTED) pr.flags |= PF_TILT_INCIDENT;
-            run_row(c, p.nx, (sl == 0 && plane) ? ROW_T_FWD : ROW_INV_T_FWD, pr, nw, p.ny, st);
-            pa.tw = s.tw_y;
-            PassArgs pc = pa;
-            if (c->inject == MS_INJECT_WAIT_TIMEOUT) pc.flags |= PF_TEST_WAIT;
-            run_col(c, p.ny, COL_STEP, pc, nw, p.nx, st);
+        auto slices = [&] {
+            PassArgs q = pa;
+            for (int sl = 0; sl < sl_end; sl++) {
+                pc.wait(c, sl);
+                q.slice = sl;
+                q.tw = s.tw_x;
+                PassArgs pr = q;
+                if (sl == 0 && iw == MS_IW_PLANE_TILTED) pr.flags |= PF_TILT_INCIDENT;
+                run_row(c, p.nx, (sl == 0 && plane) ? ROW_T_FWD : ROW_INV_T_FWD, pr, nw, p.ny, st);
+                q.tw = s.tw_y;
+                PassArgs pq = q;
+                if (c->inject == MS_INJECT_WAIT_TIMEOUT) pq.flags |= PF_TEST_WAIT;
+                run_col(c, p.ny, COL_STEP, pq, nw, p.nx, st);
+            }
+        };
+        if (pc.ev.size() <= 1 && sl_end > 1) {
+            // the slice loop replays from a captured graph (no potential chunks to wait for)
+            std::string key = graph_key_of(pa, nw, sl_end, iw, c->inject, nullptr, nullptr, nullptr, nullptr, -1);
+            run_graphed(c, key, slices);
+        } else {
+            slices();
         }
         if (eng) {
             for (int sl = sl_end; sl < S_max; sl++) pc.wait(c, sl);
@@ -1211,63 +1281,6 @@ int autotune_batch(ms_ctx* c, const ms_params& p, const Setup& s, const PassArgs
     return best;
 }
 
-// Launch arguments that a captured batch graph bakes in, as a byte string.
-std::string graph_key_of(const PassArgs& pa, int nb, int S, int nblk, int ndet, const void* partial,
-                         const void* Iw, const void* img, const void* thr, int npos)
-{
-    std::string k((const char*)&pa, sizeof(PassArgs));
-    const int ints[5] = {nb, S, nblk, ndet, npos};
-    const void* ptrs[4] = {partial, Iw, img, thr};
-    k.append((const char*)ints, sizeof(ints));
-    k.append((const char*)ptrs, sizeof(ptrs));
-    return k;
-}
-
-// Runs `body` (launches only) on the context stream through a cached CUDA graph: captured on
-// first use or when `key` changes, replayed otherwise.  Falls back to direct launches while
-// profiling (per-launch events), on the legacy default stream, or when the stream is already
-// being captured by the caller.
-template <class F>
-void run_graphed(ms_ctx* c, const std::string& key, F&& body)
-{
-    cudaStream_t st = c->stream;
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    bool ok = c->use_graphs && !c->profile && st != nullptr && st != cudaStreamLegacy &&
-              st != cudaStreamPerThread && cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
-              cs == cudaStreamCaptureStatusNone;
-    if (!ok) {
-        body();
-        return;
-    }
-    auto it = c->graphs.find(key);
-    if (it == c->graphs.end()) {
-        if (c->graphs.size() >= 4) c->drop_graph();   // full batches, the last partial batch, ...
-        const int64_t l0 = kernel_launches();
-        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        try {
-            body();
-        } catch (...) {
-            cudaGraph_t g = nullptr;
-            cudaStreamEndCapture(st, &g);
-            if (g) cudaGraphDestroy(g);
-            cudaGetLastError();
-            throw;
-        }
-        cudaGraph_t g = nullptr;
-        CK(cudaStreamEndCapture(st, &g));
-        cudaGraphExec_t ge = nullptr;
-        cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
-        cudaGraphDestroy(g);
-        CK(e);
-        ms_ctx::Graph gr;
-        gr.exec = ge;
-        gr.launches = kernel_launches() - l0;
-        add_kernel_launches(-gr.launches);   // captured, not run
-        it = c->graphs.emplace(key, gr).first;
-    }
-    CK(cudaGraphLaunch(it->second.exec, st));
-    add_kernel_launches(it->second.launches);
-}
 }  // namespace
 
 // General scan (run_STEM_general_simu, scan_simulator.cuh:115-183): for every phonon configuration
