@@ -268,7 +268,7 @@ class Context:
         self.check(lib().ms_set_pass_kernels(self.handle, variant))
 
     def set_tile_shape(self, shape: int) -> None:
-        """-1: autotuned per grid and batch (default); 0: wide tiles; 1: narrow tiles."""
+        """-1: autotuned per grid and batch (default); else bit 0 narrow rows, bit 1 narrow columns."""
         self.check(lib().ms_set_tile_shape(self.handle, int(shape)))
 
     @property

@@ -181,7 +181,7 @@ ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
 
 ms_status ms_set_tile_shape(ms_ctx* c, int shape)
 {
-    if (!c || shape < -1 || shape > 1) return MS_ERR_INVALID_ARG;
+    if (!c || shape < -1 || shape > 3) return MS_ERR_INVALID_ARG;
     c->tile_shape = shape;
     if (c->stream) {
         cudaSetDevice(c->device);

@@ -705,9 +705,9 @@ int l2_mode_for_waves(int nwaves, int64_t N)
 }
 
 // Tile shape of the hot passes (row step on the transmission store, column step) for a batch of
-// nw waves on an nx x ny grid: forced by ms_set_tile_shape, else the faster of the wide and the
-// narrow tiles, timed on the call's own transmission store and wave descriptors with a scratch
-// wave (two slice steps per shape, after one untimed round).  The choice is kept per device, grid
+// nw waves on an nx x ny grid: forced by ms_set_tile_shape, else the fastest of the four
+// combinations of wide and narrow row and column tiles, timed on the call's own transmission store
+// and wave descriptors with a scratch wave (two slice steps per shape, after one untimed round).  The choice is kept per device, grid
 // and batch size in the context and in the JSON cache file when one is set.
 int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, cudaStream_t st)
 {
@@ -729,7 +729,7 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, cudaStream_t st)
     float best_ms = 0.f;
     int best = TILE_WIDE;
     for (int rep = 0; rep < 2; rep++) {   // the first round warms up both shapes
-        for (int shape : {TILE_WIDE, TILE_NARROW}) {
+        for (int shape : {TILE_WIDE, TILE_NARROW_ROWS, TILE_NARROW_COLS, TILE_NARROW}) {
             pa.tile = shape;
             CK(cudaEventRecord(e0, st));
             for (int sl = 0; sl < 2; sl++) {

@@ -62,14 +62,14 @@ struct FftCfg<2048> {
 };
 
 // Narrow tiles for batches too small to fill the GPU (one 512^2 HRTEM wave has 32 wide row
-// blocks for 148 SMs): one warp of rows per row block, two columns per column block (the
-// narrowest tile a 16-byte tensor-memory-accelerator box allows).  The twiddles are then read
-// from global memory (L1) instead of being staged per block.
+// blocks for 148 SMs): one warp of rows per row block, four columns per column block (32-byte
+// row segments, one sector each; two columns, the narrowest 16-byte tensor-map box, measured
+// slower).  The twiddles are then read from global memory (L1) instead of being staged per block.
 template <int N>
 struct NarrowCfg {
     static constexpr int G = FftCfg<N>::G;
     static constexpr int ROWS = G >= 32 ? 1 : 32 / G;
-    static constexpr int TC = N < 256 ? 32 / G : 2;
+    static constexpr int TC = N < 256 ? 32 / G : 4;
 };
 
 template <int N, int ROWS_ = FftCfg<N>::ROWS, int TC_ = FftCfg<N>::TC>
@@ -100,7 +100,8 @@ using FftLayout = FftLayoutT<N>;
 template <int N>
 using NarrowLayout = FftLayoutT<N, NarrowCfg<N>::ROWS, NarrowCfg<N>::TC>;
 
-// Tile shape of the hot slice passes (PassArgs.tile)
-enum TileShape { TILE_WIDE = 0, TILE_NARROW = 1 };
+// Tile shape of the hot slice passes (PassArgs.tile): a narrow row step and a narrow column step
+// are chosen independently
+enum TileShape { TILE_WIDE = 0, TILE_NARROW_ROWS = 1, TILE_NARROW_COLS = 2, TILE_NARROW = 3 };
 
 }  // namespace msb

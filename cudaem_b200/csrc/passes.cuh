@@ -902,7 +902,7 @@ void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st
     if (op == ROW_INV_TT_FWD && a.variant == PASS_PIPELINED && ((uintptr_t)a.psi & 15) == 0 &&
         row_q<N>(a, nwaves, ny, st))
         return;
-    if (op == ROW_INV_TT_FWD && a.tile == TILE_NARROW) {
+    if (op == ROW_INV_TT_FWD && (a.tile & TILE_NARROW_ROWS)) {
         // one warp of rows per block; only the transpose scratch lives in shared memory
         using NL = NarrowLayout<N>;
         auto kern = a.l2_mode == L2_WAVES_RESIDENT ? k_row_tt<N, L2_WAVES_RESIDENT, NL>
@@ -962,7 +962,7 @@ void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st
         return;
     // the hot column step reads its tile through the tensor memory accelerator
     if (op == COL_STEP && a.variant != PASS_PIPELINED && !(a.flags & PF_FILTER_AUX)) {
-        if (a.tile == TILE_NARROW && col_step_tma<N, NarrowLayout<N>>(a, nwaves, nx, st)) return;
+        if ((a.tile & TILE_NARROW_COLS) && col_step_tma<N, NarrowLayout<N>>(a, nwaves, nx, st)) return;
         if (col_step_tma<N>(a, nwaves, nx, st)) return;
     }
     dim3 grid((unsigned)(nwaves * (nx / L::TC))), block(L::COL_THREADS);

@@ -215,13 +215,15 @@ ms_status ms_set_graphs(ms_ctx* ctx, int enable);
  * changes speed.  No reference counterpart (the reference's passes are cuFFT plans). */
 ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
 /* Tile shape of the classic hot passes (the row step on the transmission store and the column
- * step): -1 (default) autotuned per grid and batch size, 0 wide tiles (blocks of 8..16 rows or
- * 8..16 columns), 1 narrow tiles (one warp of rows, two columns per block) for batches too small
- * to fill the GPU.  The autotuner times both shapes on the call's own data the first time a grid
- * and batch size are seen.  Both shapes compute the same operations bit for bit.  No reference
- * counterpart (the reference's FFTs are cuFFT plans). */
+ * step): -1 (default) autotuned per grid and batch size; otherwise a bit mask, bit 0 narrow rows
+ * (one warp of rows per block, twiddles from L1), bit 1 narrow columns (four columns per block):
+ * 0 wide tiles (blocks of 8..16 rows or columns), 1 narrow rows, 2 narrow columns, 3 both.  Narrow
+ * tiles spread batches too small to fill the GPU over every SM.  The autotuner times the four
+ * shapes on the call's own data the first time a grid and batch size are seen.  All shapes
+ * compute the same operations bit for bit.  No reference counterpart (the reference's FFTs are
+ * cuFFT plans). */
 ms_status ms_set_tile_shape(ms_ctx* ctx, int shape);
-/* Tile shape (0 wide, 1 narrow) of the last CBED / TEM / STEM call's hot passes. */
+/* Tile shape (the bit mask above) of the last CBED / TEM / STEM call's hot passes. */
 int ms_last_tile_shape(const ms_ctx* ctx);
 /* JSON file that keeps the autotuner's choices (probe batch, tile shape) across contexts and
  * processes, keyed by device, grid and batch size; entries already in the file are loaded now.

@@ -1,11 +1,12 @@
 """Narrow tiles of the hot slice passes and the tile-shape autotuner with its JSON cache.
 
+Row and column tiles are chosen independently (a bit mask: 1 narrow rows, 2 narrow columns).
 The narrow row step (one warp of rows per block, twiddles read from global memory) and the narrow
-column step (two columns per block through a 16-byte tensor-map box) run the same transform code
+column step (four columns per block, one 32-byte sector per row) run the same transform code
 on the same twiddle values as the wide tiles, so every output is identical bit for bit.  They are
-also checked against the FP64 oracle at 128..2048 points.  The autotuner times both shapes the
-first time a grid and batch size are seen; with a cache file set, the choice is written there and
-a second context reads it back instead of timing again.
+also checked against the FP64 oracle at 128..2048 points.  The autotuner times the four
+combinations the first time a grid and batch size are seen; with a cache file set, the choice is
+written there and a second context reads it back instead of timing again.
 """
 import json
 import os
@@ -23,12 +24,12 @@ from oracle import oracle as orc  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-WIDE, NARROW = 0, 1
+WIDE, NARROW_ROWS, NARROW_COLS, NARROW = 0, 1, 2, 3
 
 
-def _shapes(ctx, fn):
+def _shapes(ctx, fn, shapes=(WIDE, NARROW)):
     out = []
-    for shape in (WIDE, NARROW):
+    for shape in shapes:
         ctx.set_tile_shape(shape)
         try:
             out.append(fn())
@@ -42,8 +43,9 @@ def _shapes(ctx, fn):
 def test_cbed_narrow_equals_wide(ctx, n, nconf):
     p, at = cases.cbed_small(n=n, cells=(3, 3, 4), nconf=nconf)
     sim = cb.MulSimulator(ctx=ctx)
-    a, b = _shapes(ctx, lambda: sim.executionCBED(p, at).image_intensity)
-    assert np.array_equal(a, b)
+    a, ar, ac, b = _shapes(ctx, lambda: sim.executionCBED(p, at).image_intensity,
+                           (WIDE, NARROW_ROWS, NARROW_COLS, NARROW))
+    assert np.array_equal(a, b) and np.array_equal(a, ar) and np.array_equal(a, ac)
     if n <= 512:
         assert rel_l2(b, orc.simulate_cbed(p, at)) < 1e-5
 
@@ -75,7 +77,7 @@ def test_rectangular_grid_narrow(ctx):
 
 def test_tile_shape_rejects_unknown_values(ctx):
     with pytest.raises(cb.MsError):
-        ctx.set_tile_shape(2)
+        ctx.set_tile_shape(4)
 
 
 def test_autotuner_cache_round_trip(tmp_path):
@@ -89,8 +91,8 @@ def test_autotuner_cache_round_trip(tmp_path):
         entries = json.load(f)
     tiles = {k: v for k, v in entries.items() if k.startswith("tile|") and k.endswith("|512,512,1")}
     assert len(tiles) == 1 and list(tiles.values())[0] == chosen
-    # a cached choice the tuner would not have made is still the one used: the file is read back
-    forced = NARROW if chosen == WIDE else WIDE
+    # a cached choice the tuner did not make is still the one used: the file is read back
+    forced = (chosen + 1) % 4
     key = next(iter(tiles))
     entries[key] = forced
     with open(path, "w") as f:
