@@ -55,6 +55,8 @@ def parse():
                          "2 persistent slice engine (every slice of a batch in one launch)")
     ap.add_argument("--potential-overlap", type=int, default=0, choices=[0, 1],
                     help="potentials: 0 all before the slice loop (default), 1 in chunks beside the slice passes")
+    ap.add_argument("--tune-cache", default="",
+                    help="JSON file keeping the autotuner's choices (probe batch, tile shape) across runs")
     ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
     ap.add_argument("--nconf", type=int, default=0, help="phonon configurations (0: the workload's)")
     return ap.parse_args()
@@ -369,11 +371,12 @@ def run_reference(args):
 
 
 # DRAM bytes (read + write) of one launch of a slice pass, from one ncu capture of the same launch
-# (8 waves of 1024^2 in flight, caches not flushed, after the same command ran without ncu):
+# (8 waves of 1024^2 in flight, caches not flushed, after the same command ran without ncu; the
+# column step with wide tiles, the row step with narrow tiles, as the autotuner picks them):
 # keyed by (workload, kernel class, grid, waves per launch)
 DRAM_TRAFFIC = {
-    ("cbed", "col", 1024, 8): 57.831936e6 + 50.721792e6,
-    ("cbed", "row", 1024, 8): 130.415360e6 + 65.834752e6,
+    ("cbed", "col", 1024, 8): 57.330944e6 + 39.807232e6,
+    ("cbed", "row", 1024, 8): 106.883840e6 + 29.984768e6,
 }
 
 
@@ -401,6 +404,8 @@ def run_ours(args):
         desc = dict(desc, workload=desc["workload"] + f" [reduced: cells_z={args.cells_z}, nconf={args.nconf}]")
     ctx = cb.Context(local)
     ctx.set_pass_kernels(args.pass_kernels)
+    if args.tune_cache:
+        ctx.set_tune_cache(args.tune_cache)
     ctx.set_potential_overlap(bool(args.potential_overlap))
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)

@@ -707,12 +707,16 @@ int l2_mode_for_waves(int nwaves, int64_t N)
 // Tile shape of the hot passes (row step on the transmission store, column step) for a batch of
 // nw waves on an nx x ny grid: forced by ms_set_tile_shape, else the fastest of the four
 // combinations of wide and narrow row and column tiles, timed on the call's own transmission store
-// and wave descriptors with a scratch wave (two slice steps per shape, after one untimed round).  The choice is kept per device, grid
-// and batch size in the context and in the JSON cache file when one is set.
-int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, cudaStream_t st)
+// (slices 0..nslices-1) and wave descriptors with a scratch wave.  Each timing covers enough slice
+// steps for about 2 ms of work (at least two), so that a single small wave is timed above the
+// event resolution; a shape's time is the best of two timed rounds after one untimed round.  The
+// choice is kept per device, grid and batch size in the context and in the JSON cache file when
+// one is set.  Under a profiler the timings are distorted: a cache file written by a plain run
+// keeps the choice of a profiled run the same.
+int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cudaStream_t st)
 {
     if (c->tile_shape >= 0) return c->tile_shape;
-    if (!pa.tt || pa.variant == PASS_PIPELINED) return TILE_WIDE;
+    if (!pa.tt || pa.variant == PASS_PIPELINED || nslices <= 0) return TILE_WIDE;
     char key[64];
     std::snprintf(key, sizeof(key), "%d,%d,%d", nx, ny, nw);
     auto it = c->tile_choice.find(key);
@@ -726,29 +730,70 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, cudaStream_t st)
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    float best_ms = 0.f;
-    int best = TILE_WIDE;
-    for (int rep = 0; rep < 2; rep++) {   // the first round warms up both shapes
-        for (int shape : {TILE_WIDE, TILE_NARROW_ROWS, TILE_NARROW_COLS, TILE_NARROW}) {
-            pa.tile = shape;
-            CK(cudaEventRecord(e0, st));
-            for (int sl = 0; sl < 2; sl++) {
-                pa.slice = sl;
-                pa.tw = twiddles(c, nx);
-                launch_row(nx, ROW_INV_T_FWD, pa, nw, ny, st);
-                pa.tw = twiddles(c, ny);
-                launch_col(ny, COL_STEP, pa, nw, nx, st);
+    constexpr int kShapes[4] = {TILE_WIDE, TILE_NARROW_ROWS, TILE_NARROW_COLS, TILE_NARROW};
+    float t_best[4] = {0.f, 0.f, 0.f, 0.f};
+    int steps = 2;
+    auto launch_steps = [&](int shape) {
+        pa.tile = shape;
+        for (int sl = 0; sl < steps; sl++) {
+            pa.slice = sl % nslices;
+            pa.tw = twiddles(c, nx);
+            launch_row(nx, ROW_INV_T_FWD, pa, nw, ny, st);
+            pa.tw = twiddles(c, ny);
+            launch_col(ny, COL_STEP, pa, nw, nx, st);
+        }
+    };
+    // The slice loops these shapes serve replay from CUDA graphs, so the timed steps replay from
+    // graphs too when the stream allows a capture: timed as direct launches, a small wave's steps
+    // are bound by the host's launch rate and every shape looks the same.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const bool graphs = c->use_graphs && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread &&
+                        cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+    cudaGraphExec_t ge[4] = {nullptr, nullptr, nullptr, nullptr};
+    struct GeFree {
+        cudaGraphExec_t* g;
+        ~GeFree()
+        {
+            for (int i = 0; i < 4; i++)
+                if (g[i]) cudaGraphExecDestroy(g[i]);
+        }
+    } ge_free{ge};
+    for (int rep = 0; rep < 3; rep++) {   // the first round warms up every shape and sizes the timings
+        for (int si = 0; si < 4; si++) {
+            if (graphs && rep == 1 && !ge[si]) {
+                const int64_t l0 = kernel_launches();
+                CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                try {
+                    launch_steps(kShapes[si]);
+                } catch (...) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(st, &g);
+                    if (g) cudaGraphDestroy(g);
+                    cudaGetLastError();
+                    throw;
+                }
+                cudaGraph_t g = nullptr;
+                CK(cudaStreamEndCapture(st, &g));
+                const cudaError_t e = cudaGraphInstantiate(&ge[si], g, 0);
+                cudaGraphDestroy(g);
+                CK(e);
+                add_kernel_launches(-(kernel_launches() - l0));   // captured, not run
             }
+            CK(cudaEventRecord(e0, st));
+            if (ge[si]) CK(cudaGraphLaunch(ge[si], st));
+            else launch_steps(kShapes[si]);
             CK(cudaEventRecord(e1, st));
             CK(cudaEventSynchronize(e1));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (rep == 1 && (shape == TILE_WIDE || ms < best_ms)) {
-                best_ms = ms;
-                best = shape;
-            }
+            if (rep == 0 && si == 0) steps = std::max(2, std::min(64, (int)(2.0 * steps / std::max(ms, 1e-3f))));
+            if (rep == 1 || (rep == 2 && ms < t_best[si])) t_best[si] = ms;
         }
     }
+    int best = TILE_WIDE;
+    for (int si = 1; si < 4; si++)
+        if (t_best[si] < t_best[best]) best = si;
+    best = kShapes[best];
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->tile_choice[key] = best;
@@ -1027,7 +1072,7 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
         pa.l2_mode = l2_mode_for_waves(nw, N);
         pa.tt = sT;
-        pa.tile = choose_tile(c, pa, p.nx, p.ny, nw, st);
+        pa.tile = choose_tile(c, pa, p.nx, p.ny, nw, g.S_cap, st);
         c->last_tile = pa.tile;
         if (iw == MS_IW_CONVERGENT) {
             pa.tw = s.tw_y;
@@ -1486,7 +1531,7 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
             pa.l2_mode = plain ? L2_DEFAULT : L2_SHARED_T;   // one transmission slice serves the whole batch
             pa.tt = sT;
             if (!plain) {
-                pa.tile = choose_tile(c, pa, p.nx, p.ny, nb, st);
+                pa.tile = choose_tile(c, pa, p.nx, p.ny, nb, S, st);
                 c->last_tile = pa.tile;
             }
             if (!plain) {
