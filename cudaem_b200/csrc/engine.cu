@@ -758,7 +758,18 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
                 if (g[i]) cudaGraphExecDestroy(g[i]);
         }
     } ge_free{ge};
-    for (int rep = 0; rep < 3; rep++) {   // the first round warms up every shape and sizes the timings
+    // round 0 warms up every shape (the first launch of a kernel also loads it); the step count of
+    // the timed rounds comes from two more steps of the wide shape, timed after that
+    for (int rep = 0; rep < 3; rep++) {
+        if (rep == 1) {
+            CK(cudaEventRecord(e0, st));
+            launch_steps(TILE_WIDE);
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            steps = std::max(2, std::min(64, (int)(2.0 * steps / std::max(ms, 1e-3f))));
+        }
         for (int si = 0; si < 4; si++) {
             if (graphs && rep == 1 && !ge[si]) {
                 const int64_t l0 = kernel_launches();
@@ -786,7 +797,6 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
             CK(cudaEventSynchronize(e1));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (rep == 0 && si == 0) steps = std::max(2, std::min(64, (int)(2.0 * steps / std::max(ms, 1e-3f))));
             if (rep == 1 || (rep == 2 && ms < t_best[si])) t_best[si] = ms;
         }
     }
