@@ -50,9 +50,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-vs-plain, adjoint and uneven-batch measurements")
-    ap.add_argument("--pass-kernels", type=int, default=0, choices=[0, 1, 2],
-                    help="slice-pass kernel form: 0 classic (default), 1 persistent pipelined, "
-                         "2 persistent slice engine (every slice of a batch in one launch)")
+    ap.add_argument("--pass-kernels", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="slice-pass kernel form: 0 classic per-slice launches, uneven batches in the slice engine "
+                         "(default); 1 persistent pipelined; 2 persistent slice engine everywhere; 3 per-slice "
+                         "launches everywhere")
     ap.add_argument("--potential-overlap", type=int, default=0, choices=[0, 1],
                     help="potentials: 0 all before the slice loop (default), 1 in chunks beside the slice passes")
     ap.add_argument("--tune-cache", default="",
@@ -190,8 +191,9 @@ def extras(ctx, pass_kernels: int = 0):
     """The metric's other two legs, the uneven batch and the HRTEM image, each device-timed through
     the C ABI: batched STEM against the one-probe-per-launch path, the adjoint against a forward
     pass, the 64-instance uneven batch with its completion-latency percentiles and its roofline,
-    and one 512^2 HRTEM image (a single wave).  The STEM batch and the uneven batch are also timed
-    in the persistent slice engine (pass-kernel form 2)."""
+    and one 512^2 HRTEM image (a single wave).  The STEM batch is also timed in the persistent slice
+    engine (pass-kernel form 2); the uneven batch runs in the engine by default and is also timed
+    with per-slice launches (form 3)."""
     import ctypes as C
 
     import torch
@@ -312,11 +314,14 @@ def extras(ctx, pass_kernels: int = 0):
                                      "sum of every instance's 20 N bytes per probe-slice"}}
 
     out["uneven_batch"] = dict(workload="64 CBED instances drawn from seed 42: grids 256^2..2048^2, 10-200 slices "
-                                        "of SrTiO3 or Si, 80-300 kV, 10-30 mrad, one phonon configuration each",
+                                        "of SrTiO3 or Si, 80-300 kV, 10-30 mrad, one phonon configuration each; "
+                                        "every grid group in one persistent slice-engine launch (the default); "
+                                        "latency = the device clock at which an instance's last wave was done",
                                **uneven(0))
-    out["uneven_batch"]["engine"] = uneven(2)
-    out["uneven_batch"]["engine"]["note"] = ("persistent slice engine (one launch per grid group); latency = the "
-                                             "device clock at which an instance's last wave was done")
+    out["uneven_batch"]["per_slice_launches"] = uneven(3)
+    out["uneven_batch"]["per_slice_launches"]["note"] = ("one row and one column launch per slice and grid group, "
+                                                         "groups on their own streams; latency = each instance's "
+                                                         "completion event")
 
     # HRTEM: one 512^2 plane wave, 40 slices, CTF image (a single wave: latency bound)
     p, at = wl.hrtem_sto()

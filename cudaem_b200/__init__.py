@@ -263,8 +263,8 @@ class Context:
         self.check(lib().ms_set_graphs(self.handle, 1 if enable else 0))
 
     def set_pass_kernels(self, variant: int) -> None:
-        """0: classic one-block-per-tile slice passes (default); 1: persistent pipelined passes;
-        2: the persistent slice engine (every slice of a batch in one launch)."""
+        """0 (default): classic per-slice passes, the slice engine for uneven batches; 1: persistent
+        pipelined passes; 2: the persistent slice engine everywhere; 3: per-slice passes everywhere."""
         self.check(lib().ms_set_pass_kernels(self.handle, variant))
 
     def set_tile_shape(self, shape: int) -> None:

@@ -169,7 +169,7 @@ int ms_last_probe_batch(const ms_ctx* c) { return c ? c->last_batch : 0; }
 
 ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
 {
-    if (!c || variant < 0 || variant > 2) return MS_ERR_INVALID_ARG;
+    if (!c || variant < 0 || variant > 3) return MS_ERR_INVALID_ARG;
     c->pass_variant = variant;
     if (c->stream) {
         cudaSetDevice(c->device);

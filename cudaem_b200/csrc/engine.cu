@@ -861,11 +861,13 @@ EngineArgs engine_plan(ms_ctx* c, const std::vector<int>& ns, int slice0, int N,
     return e;
 }
 
-// Whether the engine can run a batch: square grids (one layout serves rows and columns) and the
-// plain slice step (no stored inputs, filters or vacuum continuation).
-bool engine_fits(const ms_ctx* c, int nx, int ny, int flags)
+// Whether the engine runs a batch: selected (everywhere, or by default for an uneven batch's grid
+// groups), a square grid (one layout serves rows and columns) and the plain slice step (no stored
+// inputs, filters or vacuum continuation).
+bool engine_fits(const ms_ctx* c, int nx, int ny, int flags, bool uneven = false)
 {
-    return c->pass_variant == PASS_ENGINE && nx == ny &&
+    const bool wanted = c->pass_variant == PASS_ENGINE || (uneven && c->pass_variant == PASS_CLASSIC);
+    return wanted && nx == ny &&
            !(flags & (PF_STORE_X | PF_FILTER_AUX | PF_VACUUM_BEYOND | PF_PROP_ALWAYS | PF_TILT_INCIDENT));
 }
 
@@ -2169,7 +2171,7 @@ void sim_many(ms_ctx* c, int n, const ms_params* ps, const ms_atoms* as, ms_outp
             twiddles(c, G.ny);
             G.done_off = nwaves_all;
             for (int i : G.inst) nwaves_all += in[i].waves.size();
-            G.engine = engine_fits(c, G.nx, G.ny, 0);
+            G.engine = engine_fits(c, G.nx, G.ny, 0, true);
         }
         unsigned long long* dns = (unsigned long long*)c->buf("many_done_ns", sizeof(unsigned long long) * nwaves_all);
         CK(cudaMemsetAsync(dns, 0, sizeof(unsigned long long) * nwaves_all, st));

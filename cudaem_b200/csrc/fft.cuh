@@ -4,7 +4,7 @@
 // E = N/G points in registers, as a two-level Cooley-Tukey factorisation
 // N = E x G:
 //   1. each thread g takes x[g + G j] (j < E) and runs an E-point DFT in
-//      registers (radix-2 decimation in frequency, constant twiddles from
+//      registers (radix-4 decimation in frequency, constant twiddles from
 //      __constant__ memory, fully unrolled);
 //   2. the E outputs are multiplied by the inter-level twiddles W_N^(g k1)
 //      (a shared-memory table laid out [k1][g] so a team reads it without
@@ -156,22 +156,49 @@ __host__ __device__ constexpr int brev(int k)
     return r;
 }
 
-// In-register E-point DFT, E a power of two <= 64.  Output in bit-reversed
-// order: after the call a[brev<E>(k)] holds X[k].
+// multiply by -i (DIR < 0) or +i (DIR > 0)
+template <int DIR>
+__device__ __forceinline__ float2 mul_mi(float2 d)
+{
+    return DIR < 0 ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);
+}
+
+// In-register E-point DFT, E a power of two <= 64, by radix-4 decimation in frequency (a final
+// radix-2 stage when log2 E is odd).  A radix-4 step is two radix-2 stages with their twiddles
+// combined (W^(j+len/4) = -i W^j and W^j W^2j = W^3j), so it needs three twiddle products per four points
+// instead of four, and most of its twiddles are trivial or eighth-turn.  Output in bit-reversed
+// order, as the radix-2 form: after the call a[brev<E>(k)] holds X[k].
 template <int E, int DIR>
 __device__ __forceinline__ void dft_reg(float2 (&a)[E])
 {
+    // radix-4 steps, each equal to two radix-2 decimation-in-frequency stages (same output order):
+    // x0..x3 at j, j+q, j+2q, j+3q become (x0+x2)+(x1+x3), ((x0+x2)-(x1+x3)) W^2j,
+    // ((x0-x2) -+ i (x1-x3)) W^j, ((x0-x2) +- i (x1-x3)) W^3j with W = W_len (forward: -i first)
 #pragma unroll
-    for (int len = E; len >= 2; len >>= 1) {
-        const int half = len >> 1;
+    for (int len = E; len >= 4; len >>= 2) {
+        const int q = len >> 2;
 #pragma unroll
         for (int base = 0; base < E; base += len) {
 #pragma unroll
-            for (int j = 0; j < half; j++) {
-                float2 u = a[base + j], v = a[base + j + half];
-                a[base + j] = cadd(u, v);
-                a[base + j + half] = tw_apply<DIR>(csub(u, v), j * (64 / len));
+            for (int j = 0; j < q; j++) {
+                const float2 x0 = a[base + j], x1 = a[base + j + q], x2 = a[base + j + 2 * q], x3 = a[base + j + 3 * q];
+                const float2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<DIR>(csub(x1, x3));
+                const int m = j * (64 / len);
+                a[base + j] = cadd(t0, t2);
+                a[base + j + q] = tw_apply<DIR>(csub(t0, t2), (2 * m) & 63);
+                a[base + j + 2 * q] = tw_apply<DIR>(cadd(t1, t3), m);
+                a[base + j + 3 * q] = tw_apply<DIR>(csub(t1, t3), (3 * m) & 63);
             }
+        }
+    }
+    // a remaining radix-2 stage when log2(E) is odd
+    constexpr int LOG = (E >= 64) ? 6 : (E >= 32) ? 5 : (E >= 16) ? 4 : (E >= 8) ? 3 : (E >= 4) ? 2 : 1;
+    if constexpr (LOG % 2 == 1) {
+#pragma unroll
+        for (int base = 0; base < E; base += 2) {
+            const float2 u = a[base], v = a[base + 1];
+            a[base] = cadd(u, v);
+            a[base + 1] = csub(u, v);
         }
     }
 }

@@ -133,10 +133,13 @@ struct EngineArgs {
     long long wait_cycles;         // limit of a dependency wait (0: about one second)
 };
 
-// Kernel form of ROW_INV_T_FWD and COL_STEP: the classic one-block-per-tile kernels (two
-// resident blocks per SM, the default: measured faster on B200 at 1024^2) or the persistent
-// pipelined kernels (grids of 128..1024 points).  Both compute the same operations.
-enum PassVariant { PASS_CLASSIC = 0, PASS_PIPELINED = 1, PASS_ENGINE = 2 };
+// Kernel form of ROW_INV_T_FWD and COL_STEP.  PASS_CLASSIC (the default) launches the classic
+// one-block-per-tile kernels slice by slice for CBED / TEM / STEM (measured fastest there) and runs
+// an uneven batch's grid groups in the persistent slice engine (measured 1.35x faster there, with
+// half the completion latency); PASS_PIPELINED the persistent pipelined kernels (grids of
+// 128..1024 points); PASS_ENGINE the slice engine everywhere; PASS_PER_SLICE the classic kernels
+// everywhere.  All compute the same operations.
+enum PassVariant { PASS_CLASSIC = 0, PASS_PIPELINED = 1, PASS_ENGINE = 2, PASS_PER_SLICE = 3 };
 
 // Spatial cells of the atom binning: a ncx x ncy grid of square cells of side 1/inv_cell.
 struct CellGrid {

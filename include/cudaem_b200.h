@@ -205,7 +205,9 @@ int ms_last_probe_batch(const ms_ctx* ctx);
  * CUDA graph.  Disabled, every launch is issued directly; the results are identical. */
 ms_status ms_set_graphs(ms_ctx* ctx, int enable);
 /* Kernel form of the hot slice passes: 0 (default) the classic kernels, one block per tile
- * of rows or columns with two blocks resident per SM; 1 the persistent pipelined kernels
+ * of rows or columns, launched slice by slice for CBED / TEM / STEM, while an uneven batch's grid
+ * groups run in the persistent slice engine (form 2); 3 the classic kernels everywhere, uneven
+ * batches included; 1 the persistent pipelined kernels
  * (one block per SM walking the work items, the next item's wave prefetched while the
  * current one is transformed) for grids of 128..1024 points per axis; 2 the persistent slice
  * engine: on square grids, every slice of a CBED / TEM / STEM batch or of an uneven batch's
@@ -213,7 +215,7 @@ ms_status ms_set_graphs(ms_ctx* ctx, int enable);
  * and wait (bounded) for each wave's earlier items through per-wave slice counters.  All
  * forms compute the same operations (results agree to float rounding); the choice only
  * changes speed.  No reference counterpart (the reference's passes are cuFFT plans). */
-ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);
+ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);   /* 0..3 */
 /* Tile shape of the classic hot passes (the row step on the transmission store and the column
  * step): -1 (default) autotuned per grid and batch size; otherwise a bit mask, bit 0 narrow rows
  * (one warp of rows per block, twiddles from L1), bit 1 narrow columns (four columns per block):

@@ -29,6 +29,7 @@ from oracle import oracle as orc  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 ENGINE = 2
+PER_SLICE = 3
 TOL_SAME = 1e-6
 TOL_ORACLE = 1e-5
 
@@ -111,6 +112,7 @@ def test_uneven_batch_engine(ctx):
     p.ly = p.ly / 2
     jobs.append((p, at))
     sim = cb.MulSimulator(ctx=ctx)
+    ctx.set_pass_kernels(PER_SLICE)
     outs_ref, _ = sim.executionMany(jobs)
     ctx.set_pass_kernels(ENGINE)
     try:
@@ -125,6 +127,21 @@ def test_uneven_batch_engine(ctx):
     # the 128^2 group: the instance with fewer slices is done first
     assert outs[2].n_slices < outs[3].n_slices
     assert lat[2] <= lat[3]
+
+
+def test_uneven_batch_default_is_the_engine(ctx):
+    """By default the uneven batch runs its square grid groups in the engine: identical to form 2."""
+    jobs = [wl.cbed_si(cells=(2, 2, 3), n=256, nconf=2, seed=s) for s in (1, 2)]
+    jobs.append(wl.cbed_si(cells=(2, 2, 5), n=512, nconf=1, seed=3))
+    sim = cb.MulSimulator(ctx=ctx)
+    a = [o.image_intensity for o in sim.executionMany(jobs)[0]]
+    ctx.set_pass_kernels(ENGINE)
+    try:
+        b = [o.image_intensity for o in sim.executionMany(jobs)[0]]
+    finally:
+        ctx.set_pass_kernels(0)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
 
 
 def test_engine_wait_runs_out_and_context_recovers(ctx):
