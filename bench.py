@@ -291,19 +291,37 @@ def extras(ctx, pass_kernels: int = 0):
     jobs = wl.uneven_mix(64)
     peak, peak_kind = peaks()
 
+    # the patterns stay in HBM (device outputs allocated once), as in the headline metric: host
+    # outputs would add pageable copies whose cost depends on whether the host pages are mapped yet
+    nj = len(jobs)
+    ucp = (abi.ms_params * nj)()
+    uca = (abi.ms_atoms * nj)()
+    uco = (abi.ms_output * nj)()
+    keep = []
+    for i, (p_i, a_i) in enumerate(jobs):
+        C.memmove(C.byref(ucp[i]), C.byref(p_i.c()), C.sizeof(abi.ms_params))
+        uca[i] = a_i.c()
+        keep.append(a_i)
+        t = torch.empty((p_i.ny, p_i.nx), dtype=torch.float32, device="cuda")
+        keep.append(t)
+        uco[i].image_intensity = C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_float))
+        uco[i].on_device = 1
+    ulat = np.zeros(nj, np.float64)
+
     def uneven(variant):
         ctx.set_pass_kernels(variant)
-        sim.executionMany(jobs)
         best = None
-        for _ in range(2):
-            outs, lat = sim.executionMany(jobs)
-            if best is None or ctx.last_device_ms < best[0]:
-                best = (ctx.last_device_ms, outs, lat)
+        for rep in range(3):
+            ctx.check(L.ms_simulate_many(ctx.handle, nj, ucp, uca, uco,
+                                         ulat.ctypes.data_as(C.POINTER(C.c_double))))
+            if rep > 0 and (best is None or ctx.last_device_ms < best[0]):
+                best = (ctx.last_device_ms, ulat.copy())
         ctx.set_pass_kernels(pass_kernels)
-        ms, outs, lat = best
-        units = sum(o.n_slices * max(1, p.pn_nconf) for (p, _), o in zip(jobs, outs))
+        ms, lat = best
+        ns = [uco[i].n_slices for i in range(nj)]
+        units = sum(n_i * max(1, p.pn_nconf) for (p, _), n_i in zip(jobs, ns))
         # algorithmic bytes: per probe-slice 16 N (wave read + write) + 4 N (the instance's sigma V)
-        algo = sum(20.0 * p.nx * p.ny * o.n_slices * max(1, p.pn_nconf) for (p, _), o in zip(jobs, outs))
+        algo = sum(20.0 * p.nx * p.ny * n_i * max(1, p.pn_nconf) for (p, _), n_i in zip(jobs, ns))
         gbs = algo / (ms / 1e3) / 1e9
         return {"unit": "probe*slice/s", "value": units / (ms / 1e3), "ms": ms, "probe_slices": units,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
