@@ -707,7 +707,7 @@ int l2_mode_for_waves(int nwaves, int64_t N)
 // Tile shape of the hot passes (row step on the transmission store, column step) for a batch of
 // nw waves on an nx x ny grid: forced by ms_set_tile_shape, else the fastest of the four
 // combinations of wide and narrow row and column tiles, timed on the call's own transmission store
-// (slices 0..nslices-1) and wave descriptors with a scratch wave.  Each timing covers enough slice
+// (slices 0..nslices-1), wave descriptors and wave buffer, before the wave is set up.  Each timing covers enough slice
 // steps for about 2 ms of work (at least two), so that a single small wave is timed above the
 // event resolution; a shape's time is the best of two timed rounds after one untimed round.  The
 // choice is kept per device, grid and batch size in the context and in the JSON cache file when
@@ -722,10 +722,8 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
     auto it = c->tile_choice.find(key);
     if (it != c->tile_choice.end()) return it->second;
     if (c->profile) return TILE_WIDE;   // per-launch events would time the events
-    const int64_t N = (int64_t)nx * ny;
-    float2* scratch = (float2*)c->buf("tune_psi", sizeof(float2) * N * nw);
-    CK(cudaMemsetAsync(scratch, 0, sizeof(float2) * N * nw, st));
-    pa.psi = scratch;
+    // the steps run on the call's own wave buffer (pa.psi), before the probe or the plane wave
+    // is written into it: every caller fills the buffer completely before its slice loop reads it
     pa.flags = 0;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
