@@ -860,12 +860,13 @@ EngineArgs engine_plan(ms_ctx* c, const std::vector<int>& ns, int slice0, int N,
 }
 
 // Whether the engine runs a batch: selected (everywhere, or by default for an uneven batch's grid
-// groups), a square grid (one layout serves rows and columns) and the plain slice step (no stored
-// inputs, filters or vacuum continuation).
+// groups), a square grid (one layout serves rows and columns), the plain slice step (no stored
+// inputs, filters or vacuum continuation), and tensor-map encoding (its column items' tile loads);
+// otherwise the batch runs slice by slice.
 bool engine_fits(const ms_ctx* c, int nx, int ny, int flags, bool uneven = false)
 {
     const bool wanted = c->pass_variant == PASS_ENGINE || (uneven && c->pass_variant == PASS_CLASSIC);
-    return wanted && nx == ny &&
+    return wanted && nx == ny && tensor_maps_available() &&
            !(flags & (PF_STORE_X | PF_FILTER_AUX | PF_VACUUM_BEYOND | PF_PROP_ALWAYS | PF_TILT_INCIDENT));
 }
 
@@ -1290,7 +1291,7 @@ int autotune_batch(ms_ctx* c, const ms_params& p, const Setup& s, const PassArgs
     char key[96];
     std::snprintf(key, sizeof(key), "%d,%d,%d,%d", p.nx, p.ny, std::min(S, 2), hi);
     auto it = c->batch_choice.find(key);
-    if (it != c->batch_choice.end()) return it->second;
+    if (it != c->batch_choice.end()) return std::max(1, std::min(it->second, hi));
     cudaStream_t st = c->stream;
     const int bmax = cand.back();
     std::vector<WaveInfo> wv((size_t)bmax, w0);

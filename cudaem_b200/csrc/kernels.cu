@@ -47,7 +47,7 @@ void smem_attr_raw(const void* kernel, size_t bytes)
 
 // cuTensorMapEncodeTiled, looked up once through the runtime's driver entry points (the library
 // does not link the driver library).
-bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
@@ -59,6 +59,14 @@ bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int 
             encode = (PFN_cuTensorMapEncodeTiled_v12000)f;
         cudaGetLastError();
     });
+    return encode;
+}
+
+bool tensor_maps_available() { return tensor_map_encoder() != nullptr; }
+
+bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows)
+{
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
     if (!encode) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)2 * nx, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)2 * nx * sizeof(float)};

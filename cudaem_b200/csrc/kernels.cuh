@@ -195,6 +195,7 @@ bool launch_slice_engine(int N, int rowop, const PassArgs& a, const EngineArgs& 
 // rows of one engine row item and columns of one column item at transform length N
 int engine_rows(int N);
 int num_sms();   // streaming multiprocessors of the current device
+bool tensor_maps_available();   // the driver offers tensor-map encoding (TMA tile loads)
 int engine_cols(int N);
 void launch_col(int N, int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st);
 size_t row_smem(int N);

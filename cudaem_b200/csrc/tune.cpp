@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cctype>
+#include <exception>
 #include <cstdio>
 #include <fstream>
 #include <map>
@@ -42,7 +43,13 @@ std::map<std::string, long> parse_flat(const std::string& text)
         size_t k = j;
         if (k < n && (text[k] == '-' || text[k] == '+')) k++;
         while (k < n && std::isdigit((unsigned char)text[k])) k++;
-        if (k > j && std::isdigit((unsigned char)text[k - 1])) out[key] = std::stol(text.substr(j, k - j));
+        if (k > j && std::isdigit((unsigned char)text[k - 1])) {
+            try {
+                out[key] = std::stol(text.substr(j, k - j));
+            } catch (const std::exception&) {
+                // a value out of range: the entry is dropped
+            }
+        }
         i = k > j ? k : j + 1;
     }
     return out;
@@ -79,8 +86,9 @@ void tune_load(ms_ctx* c)
         const size_t a = k.find('|'), b = a == std::string::npos ? a : k.find('|', a + 1);
         if (b == std::string::npos || k.compare(a + 1, b - a - 1, tag) != 0) continue;
         const std::string kind = k.substr(0, a), rest = k.substr(b + 1);
-        if (kind == "batch") c->batch_choice[rest] = (int)kv.second;
-        else if (kind == "tile") c->tile_choice[rest] = (int)kv.second;
+        // values outside the choices the tuner makes are dropped (an edited or damaged file)
+        if (kind == "batch" && kv.second >= 1 && kv.second <= 256) c->batch_choice[rest] = (int)kv.second;
+        else if (kind == "tile" && kv.second >= 0 && kv.second <= 3) c->tile_choice[rest] = (int)kv.second;
     }
 }
 
