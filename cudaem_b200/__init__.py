@@ -267,6 +267,10 @@ class Context:
         pipelined passes; 2: the persistent slice engine everywhere; 3: per-slice passes everywhere."""
         self.check(lib().ms_set_pass_kernels(self.handle, variant))
 
+    def set_transmission_store(self, enable: bool) -> None:
+        """True (default): slices kept as t = exp(i sigma V); False: as sigma V (t formed in the row step)."""
+        self.check(lib().ms_set_transmission_store(self.handle, 1 if enable else 0))
+
     def set_tile_shape(self, shape: int) -> None:
         """-1: autotuned per grid and batch (default); else bit 0 narrow rows, bit 1 narrow columns."""
         self.check(lib().ms_set_tile_shape(self.handle, int(shape)))

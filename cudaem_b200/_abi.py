@@ -155,6 +155,7 @@ PROTOTYPES = {
     "ms_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_set_pass_kernels": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int]),
+    "ms_set_transmission_store": (C.c_int, [C.c_void_p, C.c_int]),
     "ms_last_tile_shape": (C.c_int, [C.c_void_p]),
     "ms_set_tune_cache": (C.c_int, [C.c_void_p, C.c_char_p]),
     "ms_set_potential_overlap": (C.c_int, [C.c_void_p, C.c_int]),

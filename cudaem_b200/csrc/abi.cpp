@@ -179,6 +179,18 @@ ms_status ms_set_pass_kernels(ms_ctx* c, int variant)
     return MS_OK;
 }
 
+ms_status ms_set_transmission_store(ms_ctx* c, int enable)
+{
+    if (!c || enable < 0 || enable > 1) return MS_ERR_INVALID_ARG;
+    c->trans_store = enable != 0;
+    if (c->stream) {
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+    }
+    c->drop_graph();
+    return MS_OK;
+}
+
 ms_status ms_set_tile_shape(ms_ctx* c, int shape)
 {
     if (!c || shape < -1 || shape > 3) return MS_ERR_INVALID_ARG;

@@ -39,6 +39,7 @@ struct ms_ctx {
     bool use_graphs = true;
     int pass_variant = 0;                        // msb::PassVariant of the slice-pass kernels (0: classic)
     bool pot_overlap = false;                    // potential chunks on a side stream beside the slice passes
+    bool trans_store = true;                     // CBED/TEM/STEM slices as t = exp(iσV) (else as σV)
     int last_batch = 0;                          // probe batch used by the last STEM call
     std::vector<cudaStream_t> side;              // streams of the grid groups of an uneven batch
     cudaStream_t pot_stream = nullptr;           // potential chunks computed beside the slice passes

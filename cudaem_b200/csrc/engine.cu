@@ -716,7 +716,7 @@ int l2_mode_for_waves(int nwaves, int64_t N)
 int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cudaStream_t st)
 {
     if (c->tile_shape >= 0) return c->tile_shape;
-    if (!pa.tt || pa.variant == PASS_PIPELINED || nslices <= 0) return TILE_WIDE;
+    if ((!pa.tt && !pa.sV) || pa.variant == PASS_PIPELINED || nslices <= 0) return TILE_WIDE;
     char key[64];
     std::snprintf(key, sizeof(key), "%d,%d,%d", nx, ny, nw);
     auto it = c->tile_choice.find(key);
@@ -1059,14 +1059,16 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         if (g0 == 0) ns_first = g.ns[0];
         const int nw = g.nconf;
         const int64_t slot = (int64_t)g.S_cap * N;
-        float2* sT = (float2*)c->buf("sT", sizeof(float2) * slot * nw);
+        // the slices as a transmission store t = exp(iσV) (8 bytes per pixel, formed once per pixel in
+        // the potential kernel) or as a σV store (4 bytes, t formed in the row step)
+        float2* sT = c->trans_store ? (float2*)c->buf("sT", sizeof(float2) * slot * nw) : nullptr;
+        float* sVs = c->trans_store ? nullptr : (float*)c->buf("sVs", sizeof(float) * slot * nw);
         // Potentials of every slice before the loop (default), or, with the overlap switched on, in
         // chunks of kPotChunk slices: the first on the context stream, the rest on a side stream while
         // the slice passes of earlier slices run; the row pass of the first slice of each chunk then
         // waits for that chunk's event.  With per-launch profiling on, all run in order.
-        PotChunks pc = launch_potential_chunks(c, with_transmission(pot_args(p, s, A, g, nullptr, slot, 0, g.S_cap, 0),
-                                                                    sT, s),
-                                               nw, g.S_cap);
+        const PotArgs pa0 = pot_args(p, s, A, g, sVs, slot, 0, g.S_cap, 0);
+        PotChunks pc = launch_potential_chunks(c, sT ? with_transmission(pa0, sT, s) : pa0, nw, g.S_cap);
         std::vector<WaveInfo> wv(nw);
         for (int i = 0; i < nw; i++) {
             wv[i].px = p.iw_x;
@@ -1080,7 +1082,7 @@ void sim_tem_like(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* o
         WaveInfo* dwv = (WaveInfo*)c->buf("waves", sizeof(WaveInfo) * nw);
         CK(cudaMemcpyAsync(dwv, wv.data(), sizeof(WaveInfo) * nw, cudaMemcpyHostToDevice, st));
         float2* psi = (float2*)c->buf("psi", sizeof(float2) * N * nw);
-        PassArgs pa = pass_args(s, psi, dwv, nullptr, slot, cond);
+        PassArgs pa = pass_args(s, psi, dwv, sVs, slot, cond);
         pa.l2_mode = l2_mode_for_waves(nw, N);
         pa.tt = sT;
         pa.tile = choose_tile(c, pa, p.nx, p.ny, nw, g.S_cap, st);
@@ -1504,8 +1506,13 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
         const int S = g.ns[0];
         const double cc10 = gate_coef(-kPi * (p.cond_lens.c10 + g.z_init[0]) * s.ph.lambda);
         float2* sT;
+        float* sVs = nullptr;   // σV store instead of the transmission store (ms_set_transmission_store)
         int64_t slot = (int64_t)S * N;
-        if (!plain) {
+        if (!plain && !c->trans_store) {
+            sT = nullptr;
+            sVs = (float*)c->buf("sVs", sizeof(float) * slot);
+            run_potential(c, pot_args(p, s, A, g, sVs, slot, 0, S, 0), 1, st);
+        } else if (!plain) {
             sT = (float2*)c->buf("sT", sizeof(float2) * slot);
             run_potential(c, with_transmission(pot_args(p, s, A, g, nullptr, slot, 0, S, 0), sT, s), 1, st);
         } else {
@@ -1538,7 +1545,7 @@ void sim_stem(ms_ctx* c, const ms_params& p, const ms_atoms& a, ms_output* out)
         for (int start = 0; start < npos; start += B) {
             const int nb = std::min(B, npos - start);
             CK(cudaMemcpyAsync(dwv, dwv_all + start, sizeof(WaveInfo) * nb, cudaMemcpyDeviceToDevice, st));
-            PassArgs pa = pass_args(s, psi, dwv, nullptr, plain ? 0 : slot, cond);
+            PassArgs pa = pass_args(s, psi, dwv, sVs, plain ? 0 : slot, cond);
             pa.l2_mode = plain ? L2_DEFAULT : L2_SHARED_T;   // one transmission slice serves the whole batch
             pa.tt = sT;
             if (!plain) {

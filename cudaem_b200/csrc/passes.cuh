@@ -156,8 +156,10 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
 // eviction priorities of PassArgs.l2_mode, a template argument MODE (a policy chosen at run time
 // costs the registers that make the kernel spill).
 // L is the tile layout: FftLayout<N> (wide, the default) or NarrowLayout<N> (one warp of rows per
-// block, twiddles read from global memory).
-template <int N, int MODE, class L = FftLayout<N>>
+// block, twiddles read from global memory).  SV: the slice is a σV store (the wave's own, WaveInfo.sV,
+// or the configuration's slot of PassArgs.sV) and t = exp(iσV) is formed here from the exp table
+// (read through L1), as k_row's ROW_INV_T_FWD does: the same values as a transmission store.
+template <int N, int MODE, class L = FftLayout<N>, bool SV = false>
 __global__ void __launch_bounds__(L::ROW_THREADS, L::ROW_MINB) k_row_tt(PassArgs a)
 {
     constexpr int G = L::G, E = L::E;
@@ -192,12 +194,18 @@ __global__ void __launch_bounds__(L::ROW_THREADS, L::ROW_MINB) k_row_tt(PassArgs
     team_fft<N, G, -1>(v, g, tw, scr, sync);
     conj_all(v);
     if (!beyond) {
-        const int slot = opaque(a.waves + b)->conf_slot;
-        const float2* tr = opaque(a.tt) + (size_t)slot * a.sV_slot_stride +
-                           ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N + g;
-        const uint64_t pol = l2_policy_trans(MODE);
+        const WaveInfo* wi = opaque(a.waves + b);
+        const size_t voff = ((size_t)(a.slice - a.sV_slice_base) * ny + r) * N + g;
+        if constexpr (SV) {
+            const float* vr = (wi->sV ? wi->sV : opaque(a.sV) + (size_t)wi->conf_slot * a.sV_slot_stride) + voff;
 #pragma unroll
-        for (int j = 0; j < E; j++) v[j] = cmul(v[j], ld_nc_l2hint(tr + G * j, pol));
+            for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + G * j), a.exptab));
+        } else {
+            const float2* tr = opaque(a.tt) + (size_t)wi->conf_slot * a.sV_slot_stride + voff;
+            const uint64_t pol = l2_policy_trans(MODE);
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = cmul(v[j], ld_nc_l2hint(tr + G * j, pol));
+        }
     }
     team_fft<N, G, -1>(v, g, tw, scr, sync);
     float2* dst = opaque(a.psi) + ((size_t)b * ny + r) * N + g;
@@ -911,6 +919,26 @@ void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st
         const size_t nsm = sizeof(float2) * (size_t)NL::ROWS * NL::SCR_STRIDE_ROW;
         smem_attr(kern, nsm);
         kern<<<(unsigned)(nwaves * (ny / NL::ROWS)), NL::ROW_THREADS, nsm, st>>>(a);
+        return;
+    }
+    if (op == ROW_INV_T_FWD) {
+        // the row step on a σV store in the lean kernel (wide or narrow tiles; the wave stores keep
+        // the L2 mode's priority)
+        if (a.tile & TILE_NARROW_ROWS) {
+            using NL = NarrowLayout<N>;
+            auto kern = a.l2_mode == L2_WAVES_RESIDENT ? k_row_tt<N, L2_WAVES_RESIDENT, NL, true>
+                        : a.l2_mode == L2_SHARED_T     ? k_row_tt<N, L2_SHARED_T, NL, true>
+                                                       : k_row_tt<N, L2_DEFAULT, NL, true>;
+            const size_t nsm = sizeof(float2) * (size_t)NL::ROWS * NL::SCR_STRIDE_ROW;
+            smem_attr(kern, nsm);
+            kern<<<(unsigned)(nwaves * (ny / NL::ROWS)), NL::ROW_THREADS, nsm, st>>>(a);
+        } else {
+            auto kern = a.l2_mode == L2_WAVES_RESIDENT ? k_row_tt<N, L2_WAVES_RESIDENT, L, true>
+                        : a.l2_mode == L2_SHARED_T     ? k_row_tt<N, L2_SHARED_T, L, true>
+                                                       : k_row_tt<N, L2_DEFAULT, L, true>;
+            smem_attr(kern, sm);
+            kern<<<grid, block, sm, st>>>(a);
+        }
         return;
     }
     switch (op) {

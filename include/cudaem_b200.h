@@ -225,6 +225,11 @@ ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);   /* 0..3 */
  * compute the same operations bit for bit.  No reference counterpart (the reference's FFTs are
  * cuFFT plans). */
 ms_status ms_set_tile_shape(ms_ctx* ctx, int shape);
+/* How CBED / TEM / STEM calls keep their slices between the potential kernel and the slice loop:
+ * 1 (default) as the transmission function t = exp(iσV) (FP32 complex, formed once per pixel in
+ * the potential kernel), 0 as σV (FP32, t formed in the row step from the same table).  Both give
+ * the same values; the choice trades the store's size and traffic against row-step arithmetic. */
+ms_status ms_set_transmission_store(ms_ctx* ctx, int enable);
 /* Tile shape (the bit mask above) of the last CBED / TEM / STEM call's hot passes. */
 int ms_last_tile_shape(const ms_ctx* ctx);
 /* JSON file that keeps the autotuner's choices (probe batch, tile shape) across contexts and

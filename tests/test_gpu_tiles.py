@@ -102,3 +102,28 @@ def test_autotuner_cache_round_trip(tmp_path):
         out2 = cb.MulSimulator(ctx=c2).executionTEM(p, at).image_intensity
         assert c2.last_tile_shape == forced
     assert np.array_equal(out1, out2)
+
+
+@pytest.mark.parametrize("kind", ["cbed", "hrtem", "stem"])
+def test_sigma_v_store_equals_transmission_store(ctx, kind):
+    """Slices kept as sigma V, with t = exp(i sigma V) formed in the row step from the same table,
+    give the same outputs bit for bit as the transmission store, in wide and narrow row tiles."""
+    sim = cb.MulSimulator(ctx=ctx)
+    if kind == "cbed":
+        p, at = cases.cbed_small(n=256, cells=(3, 3, 4), nconf=2)
+        f = lambda: sim.executionCBED(p, at).image_intensity  # noqa: E731
+    elif kind == "hrtem":
+        p, at = cases.hrtem_small(n=256, nconf=1)
+        f = lambda: sim.executionTEM(p, at).image_intensity  # noqa: E731
+    else:
+        p, at = cases.stem_small(n=256, scan=(3, 2), nconf=1, batch=4)
+        f = lambda: sim.executionSTEM(p, at).stem_intensity  # noqa: E731
+    ref = f()
+    ctx.set_transmission_store(False)
+    try:
+        for shape in (WIDE, NARROW):
+            ctx.set_tile_shape(shape)
+            assert np.array_equal(f(), ref)
+    finally:
+        ctx.set_tile_shape(-1)
+        ctx.set_transmission_store(True)
