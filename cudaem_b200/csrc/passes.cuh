@@ -159,7 +159,9 @@ __global__ void __launch_bounds__(FftLayout<N>::ROW_THREADS, FftLayout<N>::ROW_M
 // block, twiddles read from global memory).  SV: the slice is a σV store (the wave's own, WaveInfo.sV,
 // or the configuration's slot of PassArgs.sV) and t = exp(iσV) is formed here from the exp table
 // (read through L1), as k_row's ROW_INV_T_FWD does: the same values as a transmission store.
-template <int N, int MODE, class L = FftLayout<N>, bool SV = false>
+// XS (with SV): the transmitted real-space wave t·ψ is also written to PassArgs.xs, as
+// ROW_INV_T_FWD_X does for the adjoint's checkpoints.
+template <int N, int MODE, class L = FftLayout<N>, bool SV = false, bool XS = false>
 __global__ void __launch_bounds__(L::ROW_THREADS, L::ROW_MINB) k_row_tt(PassArgs a)
 {
     constexpr int G = L::G, E = L::E;
@@ -200,6 +202,11 @@ __global__ void __launch_bounds__(L::ROW_THREADS, L::ROW_MINB) k_row_tt(PassArgs
             const float* vr = (wi->sV ? wi->sV : opaque(a.sV) + (size_t)wi->conf_slot * a.sV_slot_stride) + voff;
 #pragma unroll
             for (int j = 0; j < E; j++) v[j] = cmul(v[j], expi_tab(__ldg(vr + G * j), a.exptab));
+            if constexpr (XS) {
+                float2* xr = opaque(a.xs) + ((size_t)b * ny + r) * N + g;
+#pragma unroll
+                for (int j = 0; j < E; j++) xr[G * j] = v[j];
+            }
         } else {
             const float2* tr = opaque(a.tt) + (size_t)wi->conf_slot * a.sV_slot_stride + voff;
             const uint64_t pol = l2_policy_trans(MODE);
@@ -903,6 +910,20 @@ void row_dispatch(int op, const PassArgs& a, int nwaves, int ny, cudaStream_t st
         return;
     dim3 grid((unsigned)(nwaves * (ny / L::ROWS))), block(L::ROW_THREADS);
     size_t sm = L::ROW_SMEM;
+    if (op == ROW_INV_T_FWD && (a.flags & PF_STORE_X) && !a.tt) {
+        // the adjoint's forward step that keeps t psi: the lean kernel with the extra store
+        if (a.tile & TILE_NARROW_ROWS) {
+            using NL = NarrowLayout<N>;
+            const size_t nsm = sizeof(float2) * (size_t)NL::ROWS * NL::SCR_STRIDE_ROW;
+            smem_attr(k_row_tt<N, L2_DEFAULT, NL, true, true>, nsm);
+            k_row_tt<N, L2_DEFAULT, NL, true, true>
+                <<<(unsigned)(nwaves * (ny / NL::ROWS)), NL::ROW_THREADS, nsm, st>>>(a);
+        } else {
+            smem_attr(k_row_tt<N, L2_DEFAULT, L, true, true>, sm);
+            k_row_tt<N, L2_DEFAULT, L, true, true><<<grid, block, sm, st>>>(a);
+        }
+        return;
+    }
     if (op == ROW_INV_T_FWD && (a.flags & PF_STORE_X)) op = ROW_INV_T_FWD_X;
     else if (a.tt && op == ROW_INV_T_FWD) op = ROW_INV_TT_FWD;
     else if (a.tt && op == ROW_T_FWD) op = ROW_TT_FWD;
