@@ -193,7 +193,7 @@ ms_status ms_set_transmission_store(ms_ctx* c, int enable)
 
 ms_status ms_set_tile_shape(ms_ctx* c, int shape)
 {
-    if (!c || shape < -1 || shape > 3) return MS_ERR_INVALID_ARG;
+    if (!c || shape < -1 || shape > 7) return MS_ERR_INVALID_ARG;
     c->tile_shape = shape;
     if (c->stream) {
         cudaSetDevice(c->device);

@@ -17,6 +17,7 @@ struct ms_ctx {
     double last_ms = 0.0;
     int64_t last_launches = 0;
     std::string prop_key;                        // parameters of the cached propagator table
+    bool propT_built = false;                    // the table's transposed copy is current too
     void* exptab = nullptr;                      // exp(2 pi i k / 1024), k < 1024
     int* d_err = nullptr;                        // device word: a bounded device-side wait ran out
     int inject = 0;                              // host-side fault injection (MS_INJECT_*), for tests

@@ -24,7 +24,8 @@ inline void smem_attr(F* kernel, size_t bytes)
 int num_sms();
 // A 2-D tensor map over a wave batch seen as rows x (2 nx) floats (rows = waves x ny), with boxes of
 // box_cols floats x box_rows rows; false when the driver cannot encode it.
-bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows);
+bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows,
+                          bool swizzle64 = false);
 
 // ---------------------------------------------------------------------------
 // L2 eviction policies for the slice passes (createpolicy over the whole access) and loads /
@@ -120,6 +121,20 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, i
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
         ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
+}
+// One 2-D box from shared memory at src (aligned as the map's swizzle needs) to the tensor map's
+// (x, y), in the thread's bulk async-group; the caller commits the group and waits for it before
+// the shared memory is reused or the block exits.
+__device__ __forceinline__ void tma_store_2d(const void* map, int x, int y, const void* src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                 ::"l"(map), "r"(x), "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void tma_store_commit_and_wait()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 // default limit of a device-side wait: about one second at the B200's clock
 constexpr long long kWaitCycles = 2000000000LL;

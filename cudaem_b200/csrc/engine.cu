@@ -277,6 +277,7 @@ struct Setup {
     const float2* prop_x;
     const float2* prop_y;
     const float2* prop;
+    const float2* propT = nullptr;   // transposed propagator tables (1024-point columns), or null
     const float2* exptab;
     int64_t N;
     int variant = PASS_CLASSIC;
@@ -330,12 +331,16 @@ Setup make_setup(ms_ctx* c, const ms_params& p)
     std::snprintf(key, sizeof(key), "%d,%d,%.17g,%.17g,%.17g,%.17g,%.17g,%d", p.nx, p.ny, p.lx, p.ly, s.gc.prop_w,
                   s.gc.g0x, s.gc.g0y, p.bwl);
     float2* P = (float2*)c->buf("prop", sizeof(float2) * kPropSets * s.N);   // dithered tables
-    if (c->prop_key != key) {
+    // transposed copy for the warp-column step (1024-point columns)
+    float2* PT = p.ny == 1024 ? (float2*)c->buf("propT", sizeof(float2) * kPropSets * s.N) : nullptr;
+    if (c->prop_key != key || (PT && !c->propT_built)) {
         launch_prop_table(p.nx, p.ny, s.gc.dgx, s.gc.dgy, s.gc.g0x, s.gc.g0y, s.gc.prop_w, s.gc.alpha, s.gc.gl2,
-                          p.bwl ? 1 : 0, P, c->stream);
+                          p.bwl ? 1 : 0, P, c->stream, PT);
         c->prop_key = key;
+        c->propT_built = PT != nullptr;
     }
     s.prop = P;
+    s.propT = PT;
     if (!c->exptab) {
         std::vector<float2> e(1024);
         for (int k = 0; k < 1024; k++) {
@@ -689,6 +694,7 @@ PassArgs pass_args(const Setup& s, float2* psi, const WaveInfo* waves, const flo
     a.prop_x = s.prop_x;
     a.prop_y = s.prop_y;
     a.prop = s.prop;
+    a.propT = s.propT;
     a.exptab = s.exptab;
     a.grid = s.gd;
     a.lens = lens;
@@ -728,8 +734,12 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    constexpr int kShapes[4] = {TILE_WIDE, TILE_NARROW_ROWS, TILE_NARROW_COLS, TILE_NARROW};
-    float t_best[4] = {0.f, 0.f, 0.f, 0.f};
+    // the warp-column step joins the candidates on 1024-point columns with transposed tables
+    const bool warp_cols = ny == 1024 && pa.propT != nullptr;
+    constexpr int kShapes[6] = {TILE_WIDE, TILE_NARROW_ROWS, TILE_NARROW_COLS, TILE_NARROW, TILE_WARP_COLS,
+                                TILE_WARP_COLS | TILE_NARROW_ROWS};
+    const int nshape = warp_cols ? 6 : 4;
+    float t_best[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int steps = 2;
     auto launch_steps = [&](int shape) {
         pa.tile = shape;
@@ -747,12 +757,12 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     const bool graphs = c->use_graphs && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread &&
                         cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
-    cudaGraphExec_t ge[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaGraphExec_t ge[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     struct GeFree {
         cudaGraphExec_t* g;
         ~GeFree()
         {
-            for (int i = 0; i < 4; i++)
+            for (int i = 0; i < 6; i++)
                 if (g[i]) cudaGraphExecDestroy(g[i]);
         }
     } ge_free{ge};
@@ -768,7 +778,7 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
             CK(cudaEventElapsedTime(&ms, e0, e1));
             steps = std::max(2, std::min(64, (int)(2.0 * steps / std::max(ms, 1e-3f))));
         }
-        for (int si = 0; si < 4; si++) {
+        for (int si = 0; si < nshape; si++) {
             if (graphs && rep == 1 && !ge[si]) {
                 const int64_t l0 = kernel_launches();
                 CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -799,7 +809,7 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
         }
     }
     int best = TILE_WIDE;
-    for (int si = 1; si < 4; si++)
+    for (int si = 1; si < nshape; si++)
         if (t_best[si] < t_best[best]) best = si;
     best = kShapes[best];
     cudaEventDestroy(e0);

@@ -101,7 +101,7 @@ template <int N>
 using NarrowLayout = FftLayoutT<N, NarrowCfg<N>::ROWS, NarrowCfg<N>::TC>;
 
 // Tile shape of the hot slice passes (PassArgs.tile): a narrow row step and a narrow column step
-// are chosen independently
-enum TileShape { TILE_WIDE = 0, TILE_NARROW_ROWS = 1, TILE_NARROW_COLS = 2, TILE_NARROW = 3 };
+// are chosen independently; TILE_WARP_COLS (1024-point columns) takes one warp per column
+enum TileShape { TILE_WIDE = 0, TILE_NARROW_ROWS = 1, TILE_NARROW_COLS = 2, TILE_NARROW = 3, TILE_WARP_COLS = 4 };
 
 }  // namespace msb

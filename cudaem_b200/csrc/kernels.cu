@@ -64,7 +64,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 
 bool tensor_maps_available() { return tensor_map_encoder() != nullptr; }
 
-bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows)
+bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int box_cols, int box_rows,
+                          bool swizzle64)
 {
     const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
     if (!encode) return false;
@@ -73,7 +74,8 @@ bool encode_wave_tile_map(void* map, const void* psi, int nx, int64_t rows, int 
     const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return encode((CUtensorMap*)map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(psi), dims, strides, box,
-                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  swizzle64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -101,7 +103,7 @@ int num_sms()
 // kPropSets dithered FP32 tables (fft_layout.hpp): P holds kPropSets * nx * ny entries, table t
 // used by the slices s with s mod kPropSets = t.
 __global__ void k_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
-                             double gl2, int bwl, double inv_n, float2* P)
+                             double gl2, int bwl, double inv_n, float2* P, float2* PT)
 {
     int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y;
     if (ix >= nx) return;
@@ -112,13 +114,15 @@ __global__ void k_prop_table(int nx, int ny, double dgx, double dgy, double g0x,
     double s, c;
     sincos(th, &s, &c);
     dither_sets(amp * c, amp * s, kPropSets, P + (size_t)iy * nx + ix, (size_t)nx * ny);
+    // the same tables transposed ([set][kx][ky]) for the warp-column step
+    if (PT) dither_sets(amp * c, amp * s, kPropSets, PT + (size_t)ix * ny + iy, (size_t)nx * ny);
 }
 
 void launch_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
-                       double gl2, int bwl, float2* P, cudaStream_t st)
+                       double gl2, int bwl, float2* P, cudaStream_t st, float2* PT)
 {
     k_prop_table<<<dim3((nx + 127) / 128, ny), 128, 0, st>>>(nx, ny, dgx, dgy, g0x, g0y, w, alpha, gl2, bwl,
-                                                             1.0 / ((double)nx * ny), P);
+                                                             1.0 / ((double)nx * ny), P, PT);
     count_launch();
     check_launch("propagator table");
 }

@@ -89,7 +89,8 @@ struct PassArgs {
     const float2* tw;         // inter-level twiddles for this pass's length
     const float2* prop_x;     // [nx] exp(i w (gx - g0x)^2)
     const float2* prop_y;     // [ny] exp(i w (gy - g0y)^2)
-    const float2* prop;       // [2][ny][nx] full propagator P(k) including 1/N and the band limit, as hi + lo planes
+    const float2* prop;       // [kPropSets][ny][nx] full propagator P(k) including 1/N and the band limit (dithered)
+    const float2* propT;      // the same tables transposed, [kPropSets][nx][ny] (the warp-column step), or null
     const float2* exptab;     // [1024] exp(2 pi i k / 1024) for the transmission
     GridDev grid;
     LensDev lens;
@@ -202,7 +203,7 @@ size_t row_smem(int N);
 size_t col_smem(int N);
 void launch_potential(const PotArgs& a, int n_conf, cudaStream_t st);
 void launch_prop_table(int nx, int ny, double dgx, double dgy, double g0x, double g0y, double w, double alpha,
-                       double gl2, int bwl, float2* P, cudaStream_t st);
+                       double gl2, int bwl, float2* P, cudaStream_t st, float2* PT = nullptr);
 
 // specimen on the device
 void launch_displace(const float* x, const float* y, const float* z, const float* sig, int64_t n, const int* confs,

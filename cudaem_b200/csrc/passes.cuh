@@ -526,6 +526,111 @@ __global__ void __launch_bounds__(L::COL_THREADS, L::COL_MINB)
     for (int j = 0; j < E; j++) st_l2hint(cp + j * cs, v[j], pol);
 }
 
+// Column step with one warp per column (TILE_WARP_COLS, 1024-point columns: a team of G = 32
+// threads is one warp, so the transforms synchronise within the warp only).  The block's 8
+// columns arrive by TMA through a tensor map with the 64-byte swizzle: in a 64-byte row of the
+// tile, the 16-byte chunk c/2 of column c sits at chunk (c/2) XOR (row/2 mod 4), so a warp reading
+// one column down 32 rows touches 8 bank pairs per half-warp (a 2-way conflict) instead of 2.  The
+// propagator comes from the transposed tables (PassArgs.propT, [kx][ky]), read along the column
+// with whole-warp coalesced loads.  The results go back into the swizzled tile and out by TMA
+// stores.  The arithmetic is k_col_step_tma's (the same transforms, twiddles and products), so
+// the outputs are identical.
+template <int N>
+__global__ void __launch_bounds__(256, 2) k_col_step_warp(PassArgs a, const __grid_constant__ CUtensorMap tmap)
+{
+    using L = FftLayout<N>;
+    constexpr int G = L::G, E = L::E, TC = 8, BOX = 256;
+    static_assert(G == 32, "one team per warp");
+    constexpr int SCR = E * (G + 1) + 1;                      // one team's transposition scratch (float2)
+    constexpr unsigned TILE_BYTES = (unsigned)(N * TC * sizeof(float2));
+    static_assert((size_t)TILE_BYTES <= (size_t)TC * SCR * sizeof(float2), "the tile lives in the scratch");
+    __shared__ __align__(8) uint64_t bar;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // 1024-byte aligned base (the launch adds 1024 bytes of slack): the swizzle acts on address bits
+    unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const int nx = a.grid.nx;
+    const int tiles = nx / TC;
+    const int b = blockIdx.x / tiles;
+    const int col0 = (blockIdx.x % tiles) * TC;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const WaveInfo& wi = a.waves[b];
+    if (a.slice >= wi.n_slices && !(a.flags & PF_VACUUM_BEYOND)) return;
+    const bool final_step = (a.slice == wi.n_slices - 1) && !(a.flags & PF_PROP_ALWAYS);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, TILE_BYTES + ((a.flags & PF_TEST_WAIT) ? 16u : 0u));
+#pragma unroll
+        for (int q = 0; q < N / BOX; q++) tma_load_2d(base + q * BOX * 64, &tmap, 2 * col0, b * N + q * BOX, &bar);
+    }
+    __syncthreads();
+    const long long limit = (a.flags & PF_TEST_WAIT) ? 2000000LL : (a.wait_cycles > 0 ? a.wait_cycles : kWaitCycles);
+    const bool late = !mbar_wait_bounded(&bar, 0, limit);
+    if (__syncthreads_or(late)) {
+        if (threadIdx.x == 0 && a.err) atomicOr(a.err, 1);
+        return;
+    }
+    // element (row r, column c) of the swizzled tile
+    auto at = [base](int r, int c) {
+        return reinterpret_cast<float2*>(base + r * 64 + ((((c >> 1) ^ ((r >> 1) & 3)) << 4) | ((c & 1) << 3)));
+    };
+    float2 v[E];
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j] = *at(lane + G * j, w);
+    __syncthreads();   // every warp holds its column: the tile region becomes the scratch
+    float2* scr_base = reinterpret_cast<float2*>(base) + w * SCR;
+    auto scr = [scr_base](int k1, int q) { return scr_base + k1 * (G + 1) + q; };
+    auto sync = []() { __syncwarp(); };
+    const float2* tw = tw_set<N>(a);   // through L1
+    const int col = col0 + w;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+        team_fft<N, G, -1>(v, lane, tw, scr, sync);
+        if (pass == 1) {
+            conj_all(v);
+            break;
+        }
+        if (final_step) break;
+        const float2* pp = opaque(prop_set(a.propT, a) + (size_t)col * N + lane);
+        const uint64_t pl = l2_policy_evict_last();
+        if (a.flags & PF_CONJ_PROP) {
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = cmulc(v[j], ld_nc_l2hint(pp + G * j, pl));
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; j++) v[j] = cmul(v[j], ld_nc_l2hint(pp + G * j, pl));
+        }
+        conj_all(v);
+    }
+    __syncthreads();   // every warp is done with its scratch: the region takes the result tile
+#pragma unroll
+    for (int j = 0; j < E; j++) *at(lane + G * j, w) = v[j];
+    // the tile's ordinary stores before the tensor-memory-accelerator reads of it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < N / BOX; q++) tma_store_2d(&tmap, 2 * col0, b * N + q * BOX, base + q * BOX * 64);
+        tma_store_commit_and_wait();
+    }
+}
+
+template <int N>
+static bool col_step_warp(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
+{
+    if constexpr (N != 1024) {
+        return false;
+    } else {
+        using L = FftLayout<N>;
+        if (!a.propT || nx % 8 != 0 || ((uintptr_t)a.psi & 15) != 0) return false;
+        CUtensorMap map;
+        if (!encode_wave_tile_map(&map, a.psi, nx, (int64_t)nwaves * N, 16, 256, true)) return false;
+        constexpr size_t sm = sizeof(float2) * 8 * (L::E * (L::G + 1) + 1) + 1024;
+        smem_attr(k_col_step_warp<N>, sm);
+        k_col_step_warp<N><<<(unsigned)(nwaves * (nx / 8)), 256, sm, st>>>(a, map);
+        return true;
+    }
+}
+
 template <int N, class L = FftLayout<N>>
 static bool col_step_tma(const PassArgs& a, int nwaves, int nx, cudaStream_t st)
 {
@@ -1011,6 +1116,7 @@ void col_dispatch(int op, const PassArgs& a, int nwaves, int nx, cudaStream_t st
         return;
     // the hot column step reads its tile through the tensor memory accelerator
     if (op == COL_STEP && a.variant != PASS_PIPELINED && !(a.flags & PF_FILTER_AUX)) {
+        if ((a.tile & TILE_WARP_COLS) && col_step_warp<N>(a, nwaves, nx, st)) return;
         if ((a.tile & TILE_NARROW_COLS) && col_step_tma<N, NarrowLayout<N>>(a, nwaves, nx, st)) return;
         if (col_step_tma<N>(a, nwaves, nx, st)) return;
     }

@@ -88,7 +88,7 @@ void tune_load(ms_ctx* c)
         const std::string kind = k.substr(0, a), rest = k.substr(b + 1);
         // values outside the choices the tuner makes are dropped (an edited or damaged file)
         if (kind == "batch" && kv.second >= 1 && kv.second <= 256) c->batch_choice[rest] = (int)kv.second;
-        else if (kind == "tile" && kv.second >= 0 && kv.second <= 3) c->tile_choice[rest] = (int)kv.second;
+        else if (kind == "tile" && kv.second >= 0 && kv.second <= 7) c->tile_choice[rest] = (int)kv.second;
     }
 }
 

@@ -218,8 +218,10 @@ ms_status ms_set_graphs(ms_ctx* ctx, int enable);
 ms_status ms_set_pass_kernels(ms_ctx* ctx, int variant);   /* 0..3 */
 /* Tile shape of the classic hot passes (the row step on the transmission store and the column
  * step): -1 (default) autotuned per grid and batch size; otherwise a bit mask, bit 0 narrow rows
- * (one warp of rows per block, twiddles from L1), bit 1 narrow columns (four columns per block):
- * 0 wide tiles (blocks of 8..16 rows or columns), 1 narrow rows, 2 narrow columns, 3 both.  Narrow
+ * (one warp of rows per block, twiddles from L1), bit 1 narrow columns (four columns per block),
+ * bit 2 one warp per column (1024-point columns; swizzled tile and transposed propagator; takes
+ * precedence over bit 1): 0 wide tiles (blocks of 8..16 rows or columns), 1 narrow rows, 2 narrow
+ * columns, 3 both, 4 warp columns, 5 warp columns and narrow rows.  Narrow
  * tiles spread batches too small to fill the GPU over every SM.  The autotuner times the four
  * shapes on the call's own data the first time a grid and batch size are seen.  All shapes
  * compute the same operations bit for bit.  No reference counterpart (the reference's FFTs are

@@ -24,7 +24,7 @@ from oracle import oracle as orc  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-WIDE, NARROW_ROWS, NARROW_COLS, NARROW = 0, 1, 2, 3
+WIDE, NARROW_ROWS, NARROW_COLS, NARROW, WARP_COLS = 0, 1, 2, 3, 4
 
 
 def _shapes(ctx, fn, shapes=(WIDE, NARROW)):
@@ -46,6 +46,10 @@ def test_cbed_narrow_equals_wide(ctx, n, nconf):
     a, ar, ac, b = _shapes(ctx, lambda: sim.executionCBED(p, at).image_intensity,
                            (WIDE, NARROW_ROWS, NARROW_COLS, NARROW))
     assert np.array_equal(a, b) and np.array_equal(a, ar) and np.array_equal(a, ac)
+    if n == 1024:
+        # one warp per column (swizzled tile, transposed propagator), alone and with narrow rows
+        aw, awr = _shapes(ctx, lambda: sim.executionCBED(p, at).image_intensity, (WARP_COLS, WARP_COLS | NARROW_ROWS))
+        assert np.array_equal(a, aw) and np.array_equal(a, awr)
     if n <= 512:
         assert rel_l2(b, orc.simulate_cbed(p, at)) < 1e-5
 
@@ -56,6 +60,13 @@ def test_hrtem_narrow_equals_wide(ctx):
     a, b = _shapes(ctx, lambda: sim.executionTEM(p, at).image_intensity)
     assert np.array_equal(a, b)
     assert rel_l2(b, orc.simulate_tem(p, at)) < 1e-5
+
+
+def test_stem_warp_columns_equal_wide(ctx):
+    p, at = cases.stem_small(n=1024, cells=(8, 8, 2), scan=(3, 1), nconf=1, batch=3)
+    sim = cb.MulSimulator(ctx=ctx)
+    a, b = _shapes(ctx, lambda: sim.executionSTEM(p, at).stem_intensity, (WIDE, WARP_COLS))
+    assert np.array_equal(a, b)
 
 
 def test_stem_narrow_equals_wide(ctx):
@@ -77,7 +88,7 @@ def test_rectangular_grid_narrow(ctx):
 
 def test_tile_shape_rejects_unknown_values(ctx):
     with pytest.raises(cb.MsError):
-        ctx.set_tile_shape(4)
+        ctx.set_tile_shape(8)
 
 
 def test_autotuner_cache_round_trip(tmp_path):
