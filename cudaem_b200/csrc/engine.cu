@@ -766,8 +766,8 @@ int choose_tile(ms_ctx* c, PassArgs pa, int nx, int ny, int nw, int nslices, cud
                 if (g[i]) cudaGraphExecDestroy(g[i]);
         }
     } ge_free{ge};
-    // round 0 warms up every shape (the first launch of a kernel also loads it); the step count of
-    // the timed rounds comes from two more steps of the wide shape, timed after that
+    // the first pass over the shapes warms them up (the first launch of a kernel also loads it);
+    // the step count of the two timed passes comes from two more steps of the wide shape
     for (int rep = 0; rep < 3; rep++) {
         if (rep == 1) {
             CK(cudaEventRecord(e0, st));
