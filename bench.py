@@ -56,6 +56,9 @@ def parse():
                          "launches everywhere")
     ap.add_argument("--potential-overlap", type=int, default=0, choices=[0, 1],
                     help="potentials: 0 all before the slice loop (default), 1 in chunks beside the slice passes")
+    ap.add_argument("--tile-shape", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
+                    help="tile shape of the hot passes: -1 autotuned (default); bit 0 narrow rows, bit 1 narrow "
+                         "columns, bit 2 one warp per column (1024-point columns)")
     ap.add_argument("--tune-cache", default="",
                     help="JSON file keeping the autotuner's choices (probe batch, tile shape) across runs")
     ap.add_argument("--cells-z", type=int, default=0, help="specimen thickness in unit cells (0: the workload's)")
@@ -435,6 +438,7 @@ def run_ours(args):
     ctx.set_pass_kernels(args.pass_kernels)
     if args.tune_cache:
         ctx.set_tune_cache(args.tune_cache)
+    ctx.set_tile_shape(args.tile_shape)
     ctx.set_potential_overlap(bool(args.potential_overlap))
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
