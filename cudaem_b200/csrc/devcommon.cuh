@@ -131,6 +131,13 @@ __device__ __forceinline__ void tma_store_2d(const void* map, int x, int y, cons
                  ::"l"(map), "r"(x), "r"(y), "r"(smem_u32(src))
                  : "memory");
 }
+// the same with an L2 eviction priority (createpolicy) for the written lines
+__device__ __forceinline__ void tma_store_2d_hint(const void* map, int x, int y, const void* src, uint64_t pol)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2}], [%3], %4;"
+                 ::"l"(map), "r"(x), "r"(y), "r"(smem_u32(src)), "l"(pol)
+                 : "memory");
+}
 __device__ __forceinline__ void tma_store_commit_and_wait()
 {
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");

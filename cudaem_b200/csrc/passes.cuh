@@ -533,7 +533,7 @@ __global__ void __launch_bounds__(L::COL_THREADS, L::COL_MINB)
 // one column down 32 rows touches 8 bank pairs per half-warp (a 2-way conflict) instead of 2.  The
 // propagator comes from the transposed tables (PassArgs.propT, [kx][ky]), read along the column
 // with whole-warp coalesced loads.  The results go back into the swizzled tile and out by TMA
-// stores.  The arithmetic is k_col_step_tma's (the same transforms, twiddles and products), so
+// stores carrying the L2 mode's priority.  The arithmetic is k_col_step_tma's (the same transforms, twiddles and products), so
 // the outputs are identical.
 template <int N>
 __global__ void __launch_bounds__(256, 2) k_col_step_warp(PassArgs a, const __grid_constant__ CUtensorMap tmap)
@@ -608,8 +608,11 @@ __global__ void __launch_bounds__(256, 2) k_col_step_warp(PassArgs a, const __gr
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
+        // the wave's lines keep the L2 mode's priority (evict-last while the batch fits in L2)
+        const uint64_t pw = l2_policy_wave(a.l2_mode);
 #pragma unroll
-        for (int q = 0; q < N / BOX; q++) tma_store_2d(&tmap, 2 * col0, b * N + q * BOX, base + q * BOX * 64);
+        for (int q = 0; q < N / BOX; q++)
+            tma_store_2d_hint(&tmap, 2 * col0, b * N + q * BOX, base + q * BOX * 64, pw);
         tma_store_commit_and_wait();
     }
 }
