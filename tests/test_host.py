@@ -162,8 +162,13 @@ def test_no_device_is_reported():
     assert cb.lib().ms_create(C.byref(h), 0) == abi.MS_ERR_NO_DEVICE
 
 
-@pytest.mark.parametrize("name", ["ms_set_graphs", "ms_set_pass_kernels", "ms_set_tile_shape", "ms_set_potential_overlap",
+@pytest.mark.parametrize("name", ["ms_set_graphs", "ms_set_pass_kernels", "ms_set_tile_shape", "ms_set_transmission_store",
+                                  "ms_set_potential_overlap",
                                   "ms_set_profiling"])
 def test_context_switches_reject_a_null_context(name):
     """The context switches check their handle before touching any device state."""
     assert getattr(cb.lib(), name)(None, 1) == abi.MS_ERR_INVALID_ARG
+
+
+def test_tune_cache_rejects_a_null_context():
+    assert cb.lib().ms_set_tune_cache(None, b"tune.json") == abi.MS_ERR_INVALID_ARG
